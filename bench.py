@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: DOF-stage updates/s of the plain FP64 ES-DGSEM step on B200.
+
+Workload (the configuration the headline metric is quoted on): N=4 (5x5 LGL
+nodes) on 512x512 curved quads over [0,1]^2 mapped by x+0.03 sin(2 pi x)
+sin(2 pi y), reflecting walls, 8 seeded Gaussian bumps, lake at rest plus a
+seeded ripple, 5-stage 4th-order low-storage RK at CFL 0.4.  A step is one
+full time step (5 RK stages) over all 6,553,600 nodes; one DOF-stage update
+is one RK stage applied to one node's (h, hu, hv).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (under torchrun) every rank advances its own replica of the
+workload (the plain path has no data-path exchange on one mesh per GPU);
+value is the sum over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-stage updates/s on 1 B200: plain FP64 vs batched+learned at equal L2 error"
+UNIT = "DOF-stage updates/s"
+NEL, N_POLY, STAGES = 512, 4, 5
+# compulsory traffic of the element kernel per node and stage: q in (24 B),
+# Jinv, Y_xi, Y_eta, X_xi, X_eta, Bx, By (56 B), gRK in+out (48 B), q out (24 B)
+ELEM_BYTES_PER_NODE = 152
+# compulsory traffic of the whole stage (the above + face data once)
+STAGE_BYTES_PER_NODE = 168
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.result = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if sm:
+            self.result = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                           "samples": len(sm)}
+        return False
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per k_element launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_element_curved_lake_512_N4.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1].strip())
+    return None
+
+
+def build_problem(seed=0):
+    from esdgsem_mpiocca_b200 import problems
+    return problems.curved_lake(N=N_POLY, nel=NEL, seed=seed, ripple=0.01, steps=0)
+
+
+def workload_config(prob, extra=None):
+    c = {"workload": "curved_lake: N=4, 512x512 curved quads on [0,1]^2 (x+0.03 sin sin), walls, 8 seeded "
+                     "Gaussian bumps, lake at rest + 0.01 ripple, LS-RK4 (5 stages), CFL 0.4, ES flux NumFlux=0",
+         "elements": prob.K, "faces": prob.F, "nodes": prob.dofs(), "stages_per_step": STAGES,
+         "l2_policy": "inputs larger than L2 (q+gRK+geometry ~0.9 GB resident vs 126 MB L2), no flush",
+         "parallelism": "replica per GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_cpu_sample(prob, threads, seconds_target=15.0, max_steps=None):
+    """Oracle (C restatement of the reference kernels, OpenMP) on the full mesh."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle.oracle import OracleProblem
+    op = OracleProblem(prob)
+    t0 = time.perf_counter()
+    out = op.run(T=1e9, max_steps=1)  # one step to size the sample
+    t1 = time.perf_counter() - t0
+    n = max(1, int(seconds_target / max(t1, 1e-6)))
+    if max_steps:
+        n = min(n, max_steps)
+    t0 = time.perf_counter()
+    out = op.run(q=out["q"], T=1e9, max_steps=n)
+    el = time.perf_counter() - t0
+    return prob.dofs() * STAGES * out["steps"] / el, out["steps"], el
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        return reference_arm(args, ws, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from esdgsem_mpiocca_b200.deviceclass import Solver
+    prob = build_problem(seed=rank)
+    s = Solver(prob, device_id=local)
+    stream = torch.cuda.Stream()
+    s.dc.set_stream(stream.cuda_stream)
+    # warm-up: builds the step graph and runs W steps
+    s.run(T=1e9, max_steps=args.warmup)
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: inputs resident in HBM ----
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = s.dc.kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as ck:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            t_sim, nsteps_done = s.dc.advance(args.steps, 1e9)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = s.dc.kernel_launches() - launches0
+    ms = e0.elapsed_time(e1)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    dof_stages_rank = prob.dofs() * STAGES * args.steps
+    value = ws * dof_stages_rank / (ms_max / 1e3)
+
+    # ---- dominant kernel duration, timed live on the engine's stream ----
+    kern = time_element_kernel(s, stream, prob)
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = e2e_run(s, prob, stream, args.steps, dist, ws)
+
+    hbm, peak_kind = peaks()
+    ach = ELEM_BYTES_PER_NODE * prob.dofs() / (kern["ms"] / 1e3) / 1e9
+    traffic = profiled_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded curved_lake generator; no dataset exists)",
+        "config": workload_config(prob, {"sim_time_reached": t_sim}),
+        "roofline": {"bound": "hbm", "kernel": "k_element<5>", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                     "frac": ach / hbm, "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                     "traffic": traffic,
+                     "bytes_per_node": ELEM_BYTES_PER_NODE, "launch_ms": kern["ms"],
+                     "face_kernel_ms": kern["face_ms"],
+                     "stage": {"bytes_per_node": STAGE_BYTES_PER_NODE,
+                               "achieved": STAGE_BYTES_PER_NODE * prob.dofs() * STAGES * args.steps /
+                               (ms_max / 1e3) / 1e9}},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": ck.result,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, nst, el = run_cpu_sample(prob, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{nst} full time steps of the same 512x512 N=4 workload "
+                                          f"({el:.1f} s) with the C oracle (reference kernels restated), OpenMP"}
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def time_element_kernel(s, stream, prob, reps=10):
+    """Average duration of the dominant kernel (k_element) and of the face
+    kernel: real steps launched kernel by kernel with CUDA events recorded
+    on the stream they are launched on (esdg_profile_steps)."""
+    face_ms, elem_ms = s.dc.profile_steps(reps)
+    return {"ms": elem_ms, "face_ms": face_ms}
+
+
+def e2e_run(s, prob, stream, steps, dist, ws):
+    """copyDeviceVariables(q) + DGtimeloop(steps) + o_q.copyTo(q), host
+    buffers pinned, timed on the device around the three calls."""
+    import torch
+    qh = torch.from_numpy(prob.q0.copy()).pin_memory()
+    qo = torch.empty_like(qh).pin_memory()
+    qn, qon = qh.numpy(), qo.numpy()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        s.dc.copy_q_from_host(qn)
+        t, n = s.run(T=1e9, max_steps=steps)
+        s.dc.copy_q_to_host(qon)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t_ = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t_, op=dist.ReduceOp.MAX)
+        ms = float(t_.item())
+    assert np.isfinite(qon).all()
+    return {"value": ws * prob.dofs() * STAGES * steps / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": qh.numel() * 8 / steps, "d2h_bytes_per_step": qo.numel() * 8 / steps,
+            "calls": "esdg_copy_q_from_host + esdg_dg_timeloop + esdg_copy_q_to_host"}
+
+
+def reference_arm(args, ws, rank):
+    """The reference's CPU path for this workload, on the host's cores."""
+    if rank != 0:
+        return 0
+    prob = build_problem(seed=0)
+    threads = os.cpu_count() or 1
+    # bounded: the whole arm stays within a few minutes
+    rate, nst, el = run_cpu_sample(prob, threads, seconds_target=30.0,
+                                   max_steps=max(1, min(args.steps, 1000)))
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": ws, "steps": nst, "warmup": 1,
+            "ms_per_step": 1e3 * el / nst, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded curved_lake generator)", "impl": "reference",
+            "config": workload_config(prob),
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{nst} full time steps of the 512x512 N=4 workload ({el:.1f} s), C "
+                                       "restatement of the reference's Serial/OpenMP kernels and time loop"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main() or 0)

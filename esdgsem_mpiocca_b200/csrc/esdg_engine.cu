@@ -1,0 +1,913 @@
+// Device engine of the B200 ES-DGSEM shallow-water solver and its C ABI.
+//
+// esdg_deviceclass mirrors the reference's deviceclass (include/deviceclass.h,
+// src/deviceclass.cpp): it owns every device buffer, takes the host arrays
+// prepared by the set-up code, and runs the time loop.  Differences that are
+// design, not behaviour:
+//   * dt is computed on the device (wave-speed max by atomicMax on ordered
+//     bit patterns), so a step needs no host round trip; the step is captured
+//     once into a CUDA graph and replayed; the host polls the done flag every
+//     few steps instead of every step.
+//   * the edge gather is fused into the face-flux kernel and the volume term,
+//     surface lift and RK update into one element kernel per stage.
+//   * a non-finite wave speed stops the loop with ESDG_E_NONFINITE instead
+//     of running on with NaNs.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/esdg_b200.h"
+#include "esdg_kernels.cuh"
+#include "esdg_setup.hpp"
+
+namespace esdg {
+
+static thread_local std::string g_create_error;
+
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+// okl/GatherEdgeData/CollectEdgeData_Bottom.okl:16-134 (bathymetry traces, once per run)
+__global__ void k_collect_bottom_impl(int F, int ngl, const int* ED, const double* Bv, double* bl, double* br) {
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long)F * ngl) return;
+    const int f = (int)(gid / ngl), i = (int)(gid % ngl);
+    const int* r = ED + (long)f * 8;
+    const int n2 = ngl * ngl;
+    double vl = 0.0, vr = 0.0;
+    if (r[5] == 0) vl = Bv[(long)r[0] * n2 + trace_offset(r[2], i, ngl)];
+    if (r[6] == 0) vr = Bv[(long)r[1] * n2 + trace_offset(r[3], i, ngl)];
+    if (r[5] == -1) vl = vr;
+    if (r[6] == -1) vr = vl;
+    bl[gid] = vl;
+    br[gid] = vr;
+}
+
+
+class Engine {
+  public:
+    // configuration (initDeviceVariables / buildDeviceKernels)
+    int N = 0, ngl = 0, K = 0, F = 0, rank = 0, rkSSP = 0, ES = 1, Testcase = 0;
+    int PP = 0, AV = 0, DiscBottom = 0, PartialDry = 0, Friction = 0;
+    int NumFlux = 0, FluxDiff = 1;
+    double eps0 = 0, sigma_max = 0, sigma_min = 0, PosPresTOL = 0, geomFace = 0, g = 9.81, h0 = 0;
+    bool inited = false, copied = false, built = false;
+    int device = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    int kernels_per_step = 0;
+    size_t bytes = 0;
+    std::vector<Buf> bufs;
+
+    // device buffers
+    double *q = nullptr, *gRK = nullptr, *Qt = nullptr, *Qtmp = nullptr;
+    double *Jinv = nullptr, *Yxi = nullptr, *Yeta = nullptr, *Xxi = nullptr, *Xeta = nullptr;
+    double *Bx = nullptr, *By = nullptr, *B = nullptr, *X = nullptr, *Y = nullptr;
+    double *D = nullptr, *Dstrong = nullptr, *Dhat = nullptr, *Vinv = nullptr, *GLw = nullptr, *EleSizes = nullptr;
+    double *nx = nullptr, *ny = nullptr, *scal = nullptr, *bL = nullptr, *bR = nullptr, *SP = nullptr;
+    double *SGX = nullptr, *SGY = nullptr, *SPV = nullptr, *GX = nullptr, *GY = nullptr, *VP = nullptr;
+    int *EdgeData = nullptr;
+    int4 *ftab = nullptr, *side = nullptr;
+    DevState* st = nullptr;
+    DevState* st_host = nullptr;  // pinned mirror for polling
+    int* elem_inst = nullptr;     // null: one instance
+
+    // step graph
+    cudaGraphExec_t graph = nullptr;
+    std::vector<double> gA, gB, gC;
+    int gStages = 0;
+
+    ~Engine() { release(); }
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? ESDG_E_NOMEM : ESDG_E_CUDA;
+    }
+
+    template <class T>
+    int alloc(T** p, size_t n) {
+        if (n == 0) n = 1;
+        void* v = nullptr;
+        cudaError_t e = cudaMalloc(&v, n * sizeof(T));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+        e = cudaMemset(v, 0, n * sizeof(T));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
+        bufs.push_back({v, n * sizeof(T)});
+        bytes += n * sizeof(T);
+        *p = static_cast<T*>(v);
+        return 0;
+    }
+
+    void release() {
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        for (auto& e : pev)
+            if (e) { cudaEventDestroy(e); e = nullptr; }
+        for (auto& b : bufs) cudaFree(b.p);
+        bufs.clear();
+        bytes = 0;
+        if (st_host) { cudaFreeHost(st_host); st_host = nullptr; }
+        q = gRK = Qt = Qtmp = nullptr;
+        inited = copied = built = false;
+    }
+
+    PhysConst phys() const {
+        PhysConst c;
+        c.g = g;
+        c.half_g = 0.5 * g;
+        c.fourth_g = 0.25 * g;
+        c.geomFace = geomFace;
+        c.PosPresTOL = PosPresTOL;
+        c.eps0 = eps0;
+        c.sigmaMin = sigma_min;
+        c.sigmaMax = sigma_max;
+        c.ZeroTOL = std::pow(10.0, -5);
+        c.ES = ES;
+        return c;
+    }
+
+    int init(int N_, int K_, int F_, int rank_, int rkSSP_, int ES_, int Testcase_, double eps0_, double smax,
+             double smin, double tol, double geomface, double g_, int PP_, int AV_, int DiscBottom_, double h0_,
+             int PartialDry_, int Friction_) {
+        if (inited) release();
+        if (N_ < 1 || N_ > 7) return fail(ESDG_E_UNSUPPORTED, "N must be in 1..7");
+        if (K_ <= 0 || F_ <= 0) return fail(ESDG_E_ARG, "Nelem and Nfaces must be positive");
+        if ((long long)K_ * (N_ + 1) * (N_ + 1) * 3 > (1ll << 31) - 1)
+            return fail(ESDG_E_ARG, "Nelem*3*(N+1)^2 must fit a 32-bit int (as in the reference)");
+        if (DiscBottom_) return fail(ESDG_E_UNSUPPORTED, "DiscBottom=1 is outside the rebuilt hot path");
+        if (PartialDry_) return fail(ESDG_E_UNSUPPORTED, "PartialDryTreatment=1 is outside the rebuilt hot path");
+        if (Friction_) return fail(ESDG_E_UNSUPPORTED, "FrictionTerms=1 is outside the rebuilt hot path");
+        N = N_; ngl = N + 1; K = K_; F = F_; rank = rank_; rkSSP = rkSSP_; ES = ES_; Testcase = Testcase_;
+        eps0 = eps0_; sigma_max = smax; sigma_min = smin; PosPresTOL = tol; geomFace = geomface; g = g_;
+        PP = PP_; AV = AV_; DiscBottom = DiscBottom_; h0 = h0_; PartialDry = PartialDry_; Friction = Friction_;
+        const size_t n2 = (size_t)ngl * ngl, nn = (size_t)K * n2, nd = nn * 3, nf = (size_t)F * ngl;
+        int r = 0;
+        if ((r = alloc(&q, nd)) || (r = alloc(&gRK, nd)) || (r = alloc(&Qt, nd))) return r;
+        if (rkSSP && (r = alloc(&Qtmp, nd))) return r;
+        if ((r = alloc(&Jinv, nn)) || (r = alloc(&Yxi, nn)) || (r = alloc(&Yeta, nn)) || (r = alloc(&Xxi, nn)) ||
+            (r = alloc(&Xeta, nn)) || (r = alloc(&Bx, nn)) || (r = alloc(&By, nn)) || (r = alloc(&B, nn)) ||
+            (r = alloc(&X, nn)) || (r = alloc(&Y, nn)))
+            return r;
+        if ((r = alloc(&D, n2)) || (r = alloc(&Dstrong, n2)) || (r = alloc(&Dhat, n2)) || (r = alloc(&Vinv, n2)) ||
+            (r = alloc(&GLw, (size_t)ngl)) || (r = alloc(&EleSizes, (size_t)K)))
+            return r;
+        if ((r = alloc(&nx, nf)) || (r = alloc(&ny, nf)) || (r = alloc(&scal, nf)) || (r = alloc(&bL, nf)) ||
+            (r = alloc(&bR, nf)) || (r = alloc(&SP, nf * 3)))
+            return r;
+        if ((r = alloc(&EdgeData, (size_t)F * 8)) || (r = alloc(&ftab, (size_t)F)) || (r = alloc(&side, (size_t)K * 4)))
+            return r;
+        if (AV) {
+            if ((r = alloc(&SGX, nf * 2)) || (r = alloc(&SGY, nf * 2)) || (r = alloc(&SPV, nf * 2)) ||
+                (r = alloc(&GX, nn * 2)) || (r = alloc(&GY, nn * 2)) || (r = alloc(&VP, (size_t)K)))
+                return r;
+        }
+        if ((r = alloc(&st, (size_t)1))) return r;
+        cudaError_t e = cudaMallocHost(&st_host, sizeof(DevState));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+        // the zero fills ran on the legacy stream; order them before any
+        // copy issued on the engine's non-blocking stream
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+        inited = true;
+        return 0;
+    }
+
+    template <class T>
+    int h2d(T* dst, const T* src, size_t n, const char* name) {
+        if (!src) return fail(ESDG_E_ARG, std::string("null host array: ") + name);
+        cudaError_t e = cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, name);
+        return 0;
+    }
+
+    int copy(int PP_, int Nelem, const double* GLw_h, const double* nx_h, const double* ny_h, const double* scal_h,
+             const double* yxi_h, const double* yeta_h, const double* xxi_h, const double* xeta_h, const double* b_h,
+             const double* Bx_h, const double* By_h, const double* D_h, const double* Ds_h, const double* Dh_h,
+             const double* J_h, const double* x_h, const double* y_h, const double* q_h, const double* Es_h,
+             const double* gRK_h, const double* Qt_h, const double* Vinv_h, const int* MS_h, const int* OR_h,
+             const int* E2E_h, const int* ED_h, const int* ER_h) {
+        if (!inited) return fail(ESDG_E_ARG, "copyDeviceVariables before initDeviceVariables");
+        if (Nelem != K) return fail(ESDG_E_ARG, "Nelem differs from initDeviceVariables");
+        const size_t n2 = (size_t)ngl * ngl, nn = (size_t)K * n2, nd = nn * 3, nf = (size_t)F * ngl;
+        // Validate the connectivity on the host, so that no kernel can index
+        // outside its buffers.
+        if (!MS_h || !OR_h || !E2E_h || !ED_h || !ER_h) return fail(ESDG_E_ARG, "null connectivity table");
+        std::vector<int4> ft(F), sd((size_t)K * 4);
+        for (int f = 0; f < F; ++f) {
+            const int* r = ED_h + (size_t)f * 8;
+            const int eL = r[0], eR = r[1], sL = r[2], sR = r[3], same = r[4], cpuL = r[5], cpuR = r[6];
+            if (eL < 0 || eL >= K || sL < 0 || sL > 3) return fail(ESDG_E_ARG, "EdgeData: bad left element/side");
+            if (cpuL != 0) return fail(ESDG_E_UNSUPPORTED, "EdgeData: left processor must be this rank (0)");
+            if (cpuR == -1) {
+                ft[f] = make_int4(eL, -1, sL | (same ? 1 : 0) << 4, 0);
+            } else {
+                if (cpuR != 0) return fail(ESDG_E_UNSUPPORTED, "EdgeData: halo faces need more than one rank");
+                if (eR < 0 || eR >= K || sR < 0 || sR > 3) return fail(ESDG_E_ARG, "EdgeData: bad right element/side");
+                ft[f] = make_int4(eL, eR, sL | (sR << 2) | ((same ? 1 : 0) << 4), 0);
+            }
+            if (ER_h[f] != same) return fail(ESDG_E_ARG, "EdgeReversed differs from EdgeData orientation");
+        }
+        for (int e = 0; e < K; ++e)
+            for (int s = 0; s < 4; ++s) {
+                const size_t id = (size_t)e * 4 + s;
+                const int fc = E2E_h[id] - 1;
+                if (fc < 0 || fc >= F) return fail(ESDG_E_ARG, "ElemToEdge: face id out of range");
+                const int ms = MS_h[id], orr = OR_h[id];
+                if (ms != 1 && ms != -1) return fail(ESDG_E_ARG, "ElemEdgeMasterSlave must be +-1");
+                if (orr != 0 && orr != 1) return fail(ESDG_E_ARG, "ElemEdgeOrientation must be 0/1");
+                sd[id] = make_int4(fc, ms, orr, 0);
+            }
+        int r = 0;
+        if ((r = h2d(nx, nx_h, nf, "normalsX")) || (r = h2d(ny, ny_h, nf, "normalsY")) ||
+            (r = h2d(scal, scal_h, nf, "Scal")) || (r = h2d(Yxi, yxi_h, nn, "y_xi")) ||
+            (r = h2d(Yeta, yeta_h, nn, "y_eta")) || (r = h2d(Xxi, xxi_h, nn, "x_xi")) ||
+            (r = h2d(Xeta, xeta_h, nn, "x_eta")) || (r = h2d(B, b_h, nn, "b")) || (r = h2d(Bx, Bx_h, nn, "Bx")) ||
+            (r = h2d(By, By_h, nn, "By")) || (r = h2d(D, D_h, n2, "Dmat")) || (r = h2d(Dstrong, Ds_h, n2, "Dstrong")) ||
+            (r = h2d(Dhat, Dh_h, n2, "Dhat")) || (r = h2d(Jinv, J_h, nn, "J")) || (r = h2d(q, q_h, nd, "q")) ||
+            (r = h2d(EleSizes, Es_h, (size_t)K, "ElementSizes")) || (r = h2d(Vinv, Vinv_h, n2, "VdmInv")) ||
+            (r = h2d(EdgeData, ED_h, (size_t)F * 8, "EdgeData")) || (r = h2d(ftab, ft.data(), (size_t)F, "faces")) ||
+            (r = h2d(side, sd.data(), (size_t)K * 4, "sides")))
+            return r;
+        if (x_h && (r = h2d(X, x_h, nn, "x_phy"))) return r;
+        if (y_h && (r = h2d(Y, y_h, nn, "y_phy"))) return r;
+        if (gRK_h && (r = h2d(gRK, gRK_h, nd, "gRK"))) return r;
+        if (Qt_h && (r = h2d(Qt, Qt_h, nd, "Qt"))) return r;
+        if (PP_ && (r = h2d(GLw, GLw_h, (size_t)ngl, "GLw"))) return r;
+        if (!PP_ && GLw_h && (r = h2d(GLw, GLw_h, (size_t)ngl, "GLw"))) return r;
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copyDeviceVariables");
+        copied = true;
+        return 0;
+    }
+
+    int build(int FluxDifferencing, int NumFlux_, int rkSSP_, int AV_, int PP_, int DiscBottom_, int Testcase_) {
+        if (!inited) return fail(ESDG_E_ARG, "buildDeviceKernels before initDeviceVariables");
+        if (FluxDifferencing != 1)
+            return fail(ESDG_E_UNSUPPORTED, "FluxDifferencing=0 (standard DGSEM volume kernel) is not rebuilt");
+        if (NumFlux_ != 0 && NumFlux_ != 2 && NumFlux_ != 3)
+            return fail(ESDG_E_UNSUPPORTED, "NumFlux must be 0 (ES), 2 (Rusanov-type ES) or 3 (rotated ES)");
+        switch (Testcase_) {
+            case 1: case 8: case 88: case 89: case 6: case 32: case 90: case 91:
+                return fail(ESDG_E_UNSUPPORTED, "this Testcase needs a boundary kernel other than SolidWalls");
+            default: break;
+        }
+        if (rkSSP_ != rkSSP || AV_ != AV || PP_ != PP || DiscBottom_ != DiscBottom)
+            return fail(ESDG_E_ARG, "buildDeviceKernels flags differ from initDeviceVariables");
+        NumFlux = NumFlux_;
+        FluxDiff = FluxDifferencing;
+        built = true;
+        return 0;
+    }
+
+    // ---- kernel launchers (dispatch on ngl) ----
+    template <int NGL>
+    int launch_face(bool av_grad) {
+        FaceArgs a{F, ftab, q, nx, ny, scal, bL, bR, SP, SGX, SGY, elem_inst, st, phys()};
+        const long n = (long)F * NGL;
+        const int blocks = (int)((n + 255) / 256);
+        if (av_grad) {
+            if (NumFlux == 0) k_face_flux<NGL, 0, true><<<blocks, 256, 0, stream>>>(a);
+            else if (NumFlux == 2) k_face_flux<NGL, 2, true><<<blocks, 256, 0, stream>>>(a);
+            else k_face_flux<NGL, 3, true><<<blocks, 256, 0, stream>>>(a);
+        } else {
+            if (NumFlux == 0) k_face_flux<NGL, 0, false><<<blocks, 256, 0, stream>>>(a);
+            else if (NumFlux == 2) k_face_flux<NGL, 2, false><<<blocks, 256, 0, stream>>>(a);
+            else k_face_flux<NGL, 3, false><<<blocks, 256, 0, stream>>>(a);
+        }
+        ++launches;
+        return 0;
+    }
+
+    ElemArgs elem_args(int mode, double A, double Bc, double C, int lam, int shock) {
+        ElemArgs a;
+        a.K = K; a.Jinv = Jinv; a.Yxi = Yxi; a.Yeta = Yeta; a.Xxi = Xxi; a.Xeta = Xeta; a.Bx = Bx; a.By = By;
+        a.B = B; a.D = D; a.Dhat = Dhat; a.Dstrong = Dstrong; a.Vinv = Vinv; a.SP = SP; a.SGX = SGX; a.SGY = SGY;
+        a.SPV = SPV; a.side = side; a.q = q; a.gRK = gRK; a.Qt = Qt; a.Qtmp = Qtmp; a.GX = GX; a.GY = GY; a.VP = VP;
+        a.elem_inst = elem_inst; a.st = st; a.rkA = A; a.rkB = Bc; a.rkC = C; a.mode = mode; a.lam = lam;
+        a.shock = shock; a.c = phys();
+        return a;
+    }
+
+    template <int NGL>
+    void launch_stage(int mode, double A, double Bc, double C, bool last, bool shock_stage) {
+        using S = ElemShape<NGL>;
+        const int eb = (K + S::NE - 1) / S::NE;
+        const int lam_in_elem = (last && !PP) ? 1 : 0;
+        launch_face<NGL>(AV != 0);
+        if (!AV) {
+            k_element<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
+            ++launches;
+        } else {
+            k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0, shock_stage ? 1 : 0));
+            const long n = (long)F * NGL;
+            k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
+                                                                         elem_inst, st, geomFace);
+            k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
+            launches += 3;
+        }
+        if (PP && mode != 2) {
+            k_pospres<NGL><<<eb, S::THREADS, 0, stream>>>(K, EleSizes, GLw, Jinv, q, elem_inst, st, last ? 1 : 0,
+                                                          phys());
+            ++launches;
+        }
+    }
+
+    template <int NGL>
+    void launch_lambda() {
+        using S = ElemShape<NGL>;
+        k_lambda<NGL><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, stream>>>(K, q, elem_inst, st, phys());
+        ++launches;
+    }
+
+    template <int NGL>
+    void launch_shock() {
+        k_shock<NGL><<<(K + 7) / 8, 256, 0, stream>>>(K, q, B, Vinv, VP, elem_inst, st, phys());
+        ++launches;
+    }
+
+    template <int NGL>
+    void launch_step() {
+        if (AV) launch_shock<NGL>();
+        k_step_begin<<<1, 32, 0, stream>>>(1, st, ngl, AV);
+        ++launches;
+        if (rkSSP) {
+            // o_Qtmp.copyFrom(o_q) (src/deviceclass.cpp:933-936)
+            cudaMemcpyAsync(Qtmp, q, (size_t)K * ngl * ngl * 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+        }
+        for (int s = 0; s < gStages; ++s)
+            launch_stage<NGL>(rkSSP ? 1 : 0, gA[s], gB[s], gC[s], s == gStages - 1, s > 0);
+        k_step_end<<<1, 32, 0, stream>>>(1, st);
+        ++launches;
+    }
+
+#define ESDG_DISPATCH(NGLV, CALL)                 \
+    switch (NGLV) {                               \
+        case 2: CALL<2>(); break;                 \
+        case 3: CALL<3>(); break;                 \
+        case 4: CALL<4>(); break;                 \
+        case 5: CALL<5>(); break;                 \
+        case 6: CALL<6>(); break;                 \
+        case 7: CALL<7>(); break;                 \
+        case 8: CALL<8>(); break;                 \
+        default: break;                           \
+    }
+
+    template <int NGL>
+    void launch_bottom() {
+        k_collect_bottom_impl<<<(F * NGL + 255) / 256, 256, 0, stream>>>(F, NGL, EdgeData, B, bL, bR);
+        ++launches;
+    }
+
+    int check_ready() {
+        if (!inited || !copied || !built) return fail(ESDG_E_ARG, "call initDeviceVariables, copyDeviceVariables and buildDeviceKernels first");
+        return 0;
+    }
+
+    int capture_step_graph() {
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        const long long before = launches;
+        cudaGraph_t gr;
+        cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+        ESDG_DISPATCH(ngl, launch_step);
+        e = cudaStreamEndCapture(stream, &gr);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+        kernels_per_step = (int)(launches - before);
+        launches = before;
+        return 0;
+    }
+
+    int poll_state() {
+        cudaError_t e = cudaMemcpyAsync(st_host, st, sizeof(DevState), cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "state read-back");
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+        return 0;
+    }
+
+    // Runs up to nsteps (nsteps <= 0: until done) graph replays.
+    int run_steps(long long nsteps) {
+        const int chunk = 16;
+        long long done_steps = 0;
+        for (;;) {
+            int r = poll_state();
+            if (r) return r;
+            if (st_host->done) break;
+            long long todo = chunk;
+            if (nsteps > 0) {
+                if (done_steps >= nsteps) break;
+                todo = std::min<long long>(todo, nsteps - done_steps);
+            }
+            for (long long k = 0; k < todo; ++k) {
+                cudaError_t e = cudaGraphLaunch(graph, stream);
+                if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+                launches += kernels_per_step;
+            }
+            done_steps += todo;
+        }
+        return 0;
+    }
+
+    int timeloop(int stages, const double* A, const double* Bc, const double* C, double minEle, double CFL,
+                 double DFL, double T, int max_steps, double* t_out, int* steps_out) {
+        int r = check_ready();
+        if (r) return r;
+        if (stages <= 0 || stages > 8 || !A || !Bc || !C) return fail(ESDG_E_ARG, "bad Runge-Kutta tables");
+        gA.assign(A, A + stages); gB.assign(Bc, Bc + stages); gC.assign(C, C + stages);
+        gStages = stages;
+        DevState s0;
+        std::memset(&s0, 0, sizeof(s0));
+        s0.t = 0.0; s0.T = T; s0.minEle = minEle; s0.CFL = CFL; s0.DFL = DFL;
+        s0.max_steps = max_steps;
+        *st_host = s0;
+        cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "state upload");
+        ESDG_DISPATCH(ngl, launch_bottom);
+        ESDG_DISPATCH(ngl, launch_lambda);
+        if ((r = capture_step_graph())) return r;
+        if ((r = run_steps(max_steps > 0 ? max_steps : 0))) return r;
+        if ((r = poll_state())) return r;
+        if (t_out) *t_out = st_host->t;
+        if (steps_out) *steps_out = st_host->steps;
+        if (st_host->status == ST_NONFINITE)
+            return fail(ESDG_E_NONFINITE, "non-finite wave speed: the solution blew up (step " +
+                                              std::to_string(st_host->steps) + ")");
+        return 0;
+    }
+
+    int advance(int nsteps, double T, double* t_out, int* steps_out) {
+        int r = check_ready();
+        if (r) return r;
+        if (!graph) return fail(ESDG_E_ARG, "esdg_advance needs a previous esdg_dg_timeloop call");
+        if ((r = poll_state())) return r;
+        st_host->T = T;
+        st_host->done = 0;
+        st_host->max_steps = 0;
+        cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "state upload");
+        // Enough replays for nsteps; the step cap makes extra replays no-ops.
+        const int target = st_host->steps + nsteps;
+        st_host->max_steps = target;
+        e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "state upload");
+        for (int k = 0; k < nsteps; ++k) {
+            e = cudaGraphLaunch(graph, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+            launches += kernels_per_step;
+        }
+        if ((r = poll_state())) return r;
+        if (t_out) *t_out = st_host->t;
+        if (steps_out) *steps_out = st_host->steps;
+        if (st_host->status == ST_NONFINITE) return fail(ESDG_E_NONFINITE, "non-finite wave speed");
+        return 0;
+    }
+
+    // Real steps launched one kernel at a time with CUDA events recorded on
+    // the launching stream around the face and element launches; returns the
+    // average duration of each (for roofline reporting).
+    int prof_stage_index = -1;
+    cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    template <int NGL>
+    void launch_step_profiled(double* face_ms, double* elem_ms) {
+        if (AV) launch_shock<NGL>();
+        k_step_begin<<<1, 32, 0, stream>>>(1, st, ngl, AV);
+        ++launches;
+        if (rkSSP)
+            cudaMemcpyAsync(Qtmp, q, (size_t)K * ngl * ngl * 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+        using S = ElemShape<NGL>;
+        const int eb = (K + S::NE - 1) / S::NE;
+        for (int s = 0; s < gStages; ++s) {
+            const bool last = s == gStages - 1;
+            const int mode = rkSSP ? 1 : 0;
+            const int lam_in_elem = (last && !PP) ? 1 : 0;
+            cudaEventRecord(pev[0], stream);
+            launch_face<NGL>(AV != 0);
+            cudaEventRecord(pev[1], stream);
+            if (!AV) {
+                k_element<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
+                ++launches;
+            } else {
+                k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0, s > 0));
+                const long n = (long)F * NGL;
+                k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
+                                                                             elem_inst, st, geomFace);
+                k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
+                launches += 3;
+            }
+            cudaEventRecord(pev[2], stream);
+            if (PP) {
+                k_pospres<NGL><<<eb, S::THREADS, 0, stream>>>(K, EleSizes, GLw, Jinv, q, elem_inst, st, last ? 1 : 0,
+                                                              phys());
+                ++launches;
+            }
+            cudaEventSynchronize(pev[2]);
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, pev[0], pev[1]);
+            cudaEventElapsedTime(&b, pev[1], pev[2]);
+            *face_ms += a;
+            *elem_ms += b;
+        }
+        k_step_end<<<1, 32, 0, stream>>>(1, st);
+        ++launches;
+    }
+
+    int profile_steps(int nsteps, double* face_ms, double* elem_ms) {
+        int r = check_ready();
+        if (r) return r;
+        if (gStages <= 0) return fail(ESDG_E_ARG, "profile_steps needs a previous esdg_dg_timeloop call");
+        for (auto& e : pev)
+            if (!e && cudaEventCreate(&e) != cudaSuccess) return fail(ESDG_E_CUDA, "cudaEventCreate");
+        if ((r = poll_state())) return r;
+        st_host->done = 0;
+        st_host->max_steps = 0;
+        st_host->T = 1e300;
+        cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "state upload");
+        double f = 0, el = 0;
+        for (int k = 0; k < nsteps; ++k) {
+            switch (ngl) {
+                case 2: launch_step_profiled<2>(&f, &el); break;
+                case 3: launch_step_profiled<3>(&f, &el); break;
+                case 4: launch_step_profiled<4>(&f, &el); break;
+                case 5: launch_step_profiled<5>(&f, &el); break;
+                case 6: launch_step_profiled<6>(&f, &el); break;
+                case 7: launch_step_profiled<7>(&f, &el); break;
+                case 8: launch_step_profiled<8>(&f, &el); break;
+            }
+        }
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "profile_steps");
+        const double nl = (double)nsteps * gStages;
+        *face_ms = f / nl;
+        *elem_ms = el / nl;
+        return 0;
+    }
+
+    template <int NGL>
+    void launch_rhs() {
+        if (AV) {
+            // the step-start sensor (shock_stage=1 recomputes it from q)
+            launch_stage<NGL>(2, 0.0, 0.0, 0.0, false, true);
+        } else {
+            launch_stage<NGL>(2, 0.0, 0.0, 0.0, false, false);
+        }
+    }
+
+    int rhs(double* Qt_h, double* visc_h) {
+        int r = check_ready();
+        if (r) return r;
+        DevState s0;
+        std::memset(&s0, 0, sizeof(s0));
+        s0.T = 1.0;
+        *st_host = s0;
+        cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "state upload");
+        ESDG_DISPATCH(ngl, launch_bottom);
+        ESDG_DISPATCH(ngl, launch_rhs);
+        const size_t nd = (size_t)K * ngl * ngl * 3;
+        e = cudaMemcpyAsync(Qt_h, Qt, nd * sizeof(double), cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "Qt read-back");
+        if (AV && visc_h) {
+            e = cudaMemcpyAsync(visc_h, VP, (size_t)K * sizeof(double), cudaMemcpyDeviceToHost, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "visc read-back");
+        }
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "compute_rhs");
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "compute_rhs launch");
+        return 0;
+    }
+};
+
+}  // namespace esdg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+struct esdg_deviceclass {
+    esdg::Engine eng;
+};
+
+struct esdg_mesh {
+    esdg::Mesh m;
+    explicit esdg_mesh(int N) : m(N) {}
+};
+
+#define ESDG_GUARD(d)                                          \
+    if (!(d)) return ESDG_E_ARG;                               \
+    cudaError_t _dev_e = cudaSetDevice((d)->eng.device);       \
+    if (_dev_e != cudaSuccess) return (d)->eng.cuda_fail(_dev_e, "cudaSetDevice");
+
+extern "C" {
+
+int esdg_deviceclass_create(int rank, int device_id, esdg_deviceclass** out) {
+    if (!out) return ESDG_E_ARG;
+    *out = nullptr;
+    int dev = device_id;
+    cudaError_t e;
+    if (dev < 0) {
+        e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) { esdg::g_create_error = cudaGetErrorString(e); return ESDG_E_CUDA; }
+    }
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) { esdg::g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return ESDG_E_CUDA; }
+    esdg_deviceclass* d = new (std::nothrow) esdg_deviceclass();
+    if (!d) return ESDG_E_NOMEM;
+    d->eng.device = dev;
+    d->eng.rank = rank;
+    e = cudaStreamCreateWithFlags(&d->eng.own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        esdg::g_create_error = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
+        delete d;
+        return ESDG_E_CUDA;
+    }
+    d->eng.stream = d->eng.own_stream;
+    *out = d;
+    return ESDG_OK;
+}
+
+int esdg_init_device_variables(esdg_deviceclass* d, int N, int Nelem, int Nfaces, int rank, int rkSSP, int NEpad,
+                               int NEsurfpad, int Nedgepad, int NAvgPad, int ES, int Testcase, double epsilon_0,
+                               double sigma_max, double sigma_min, double PosPresTOL, double geomface,
+                               double g_const, int PositivityPreserving, int ArtificialViscosity, int DiscBottom,
+                               double h_0, int PartialDry, int FrictionTerms, int CalcArrivalTimes,
+                               int CreateTimeSeries, int CalcMaximumElevation) {
+    ESDG_GUARD(d);
+    (void)NEpad; (void)NEsurfpad; (void)Nedgepad; (void)NAvgPad;  // launch shapes are chosen per ngl
+    (void)CalcArrivalTimes; (void)CreateTimeSeries; (void)CalcMaximumElevation;  // analysis outputs: not rebuilt
+    return d->eng.init(N, Nelem, Nfaces, rank, rkSSP, ES, Testcase, epsilon_0, sigma_max, sigma_min, PosPresTOL,
+                       geomface, g_const, PositivityPreserving, ArtificialViscosity, DiscBottom, h_0, PartialDry,
+                       FrictionTerms);
+}
+
+int esdg_copy_device_variables(esdg_deviceclass* d, int PositivityPreserving, int Nelem, const double* GLw,
+                               const double* normalsX, const double* normalsY, const double* Scal,
+                               const double* y_xi, const double* y_eta, const double* x_xi, const double* x_eta,
+                               const double* b, const double* Bx, const double* By, const double* Dmat,
+                               const double* Dstrong, const double* Dhat, const double* J, const double* x_phy,
+                               const double* y_phy, const double* q, const double* ElementSizes, const double* gRK,
+                               const double* Qt, const double* VdmInv, const int* ElemEdgeMasterSlave,
+                               const int* ElemEdgeOrientation, const int* ElemToEdge, const int* EdgeData,
+                               const int* EdgeReversed) {
+    ESDG_GUARD(d);
+    return d->eng.copy(PositivityPreserving, Nelem, GLw, normalsX, normalsY, Scal, y_xi, y_eta, x_xi, x_eta, b, Bx,
+                       By, Dmat, Dstrong, Dhat, J, x_phy, y_phy, q, ElementSizes, gRK, Qt, VdmInv,
+                       ElemEdgeMasterSlave, ElemEdgeOrientation, ElemToEdge, EdgeData, EdgeReversed);
+}
+
+int esdg_build_device_kernels(esdg_deviceclass* d, int KernelVersion, int KernelVersionSTD, int Testcase,
+                              int FluxDifferencing, int NumFlux, int rkSSP, int ArtificialViscosity,
+                              int PositivityPreserving, int DiscBottom) {
+    ESDG_GUARD(d);
+    (void)KernelVersion; (void)KernelVersionSTD;
+    return d->eng.build(FluxDifferencing, NumFlux, rkSSP, ArtificialViscosity, PositivityPreserving, DiscBottom,
+                        Testcase);
+}
+
+int esdg_dg_timeloop(esdg_deviceclass* d, int Nelem, int Nfaces, int rkStages, const double* rkA, const double* rkB,
+                     const double* rkC, double globalMinEleSize, double CFL, double DFL, double T, int Testcase,
+                     int ArtificialViscosity, int rkSSP, int NumPlots, int NumTimeChecks, double g_const,
+                     int PlotVar, int EntropyPlot, int PositivityPreserving, int DiscBottom, int max_steps,
+                     double* t_out, int* steps_out) {
+    ESDG_GUARD(d);
+    (void)NumPlots; (void)NumTimeChecks; (void)PlotVar; (void)EntropyPlot; (void)Testcase;
+    esdg::Engine& E = d->eng;
+    if (Nelem != E.K || Nfaces != E.F) return E.fail(ESDG_E_ARG, "Nelem/Nfaces differ from initDeviceVariables");
+    if (ArtificialViscosity != E.AV || rkSSP != E.rkSSP || PositivityPreserving != E.PP || DiscBottom != E.DiscBottom)
+        return E.fail(ESDG_E_ARG, "time-loop flags differ from initDeviceVariables");
+    if (g_const != E.g) return E.fail(ESDG_E_ARG, "g_const differs from initDeviceVariables");
+    return E.timeloop(rkStages, rkA, rkB, rkC, globalMinEleSize, CFL, DFL, T, max_steps, t_out, steps_out);
+}
+
+int esdg_copy_q_to_host(esdg_deviceclass* d, double* q) {
+    ESDG_GUARD(d);
+    esdg::Engine& E = d->eng;
+    if (!E.inited || !q) return E.fail(ESDG_E_ARG, "copy_q_to_host: not initialised or null");
+    cudaError_t e = cudaMemcpyAsync(q, E.q, (size_t)E.K * E.ngl * E.ngl * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    if (e != cudaSuccess) return E.cuda_fail(e, "copy_q_to_host");
+    return ESDG_OK;
+}
+
+int esdg_copy_q_from_host(esdg_deviceclass* d, const double* q) {
+    ESDG_GUARD(d);
+    esdg::Engine& E = d->eng;
+    if (!E.inited || !q) return E.fail(ESDG_E_ARG, "copy_q_from_host: not initialised or null");
+    cudaError_t e = cudaMemcpyAsync(E.q, q, (size_t)E.K * E.ngl * E.ngl * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                    E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    if (e != cudaSuccess) return E.cuda_fail(e, "copy_q_from_host");
+    return ESDG_OK;
+}
+
+int esdg_copy_visc_to_host(esdg_deviceclass* d, double* visc) {
+    ESDG_GUARD(d);
+    esdg::Engine& E = d->eng;
+    if (!E.inited || !E.AV || !visc) return E.fail(ESDG_E_ARG, "copy_visc_to_host: AV not enabled or null");
+    cudaError_t e = cudaMemcpyAsync(visc, E.VP, (size_t)E.K * sizeof(double), cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    if (e != cudaSuccess) return E.cuda_fail(e, "copy_visc_to_host");
+    return ESDG_OK;
+}
+
+long long esdg_bytes_allocated(const esdg_deviceclass* d) { return d ? (long long)d->eng.bytes : -1; }
+
+long long esdg_kernel_launches(const esdg_deviceclass* d) { return d ? d->eng.launches : -1; }
+
+int esdg_free_occa_vars(esdg_deviceclass* d, int rkSSP, int PositivityPreserving, int ArtificialViscosity) {
+    ESDG_GUARD(d);
+    (void)rkSSP; (void)PositivityPreserving; (void)ArtificialViscosity;
+    d->eng.release();
+    return ESDG_OK;
+}
+
+int esdg_deviceclass_destroy(esdg_deviceclass* d) {
+    if (!d) return ESDG_E_ARG;
+    cudaSetDevice(d->eng.device);
+    d->eng.release();
+    if (d->eng.own_stream) cudaStreamDestroy(d->eng.own_stream);
+    delete d;
+    return ESDG_OK;
+}
+
+const char* esdg_last_error(const esdg_deviceclass* d) {
+    return d ? d->eng.err.c_str() : esdg::g_create_error.c_str();
+}
+
+int esdg_compute_rhs(esdg_deviceclass* d, double* Qt_host, double* visc_host) {
+    ESDG_GUARD(d);
+    if (!Qt_host) return d->eng.fail(ESDG_E_ARG, "null Qt");
+    return d->eng.rhs(Qt_host, visc_host);
+}
+
+int esdg_set_stream(esdg_deviceclass* d, void* cuda_stream) {
+    ESDG_GUARD(d);
+    esdg::Engine& E = d->eng;
+    E.stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : E.own_stream;
+    if (E.graph) { cudaGraphExecDestroy(E.graph); E.graph = nullptr; }
+    return ESDG_OK;
+}
+
+int esdg_profile_steps(esdg_deviceclass* d, int nsteps, double* face_ms, double* elem_ms) {
+    ESDG_GUARD(d);
+    if (nsteps <= 0 || !face_ms || !elem_ms) return d->eng.fail(ESDG_E_ARG, "bad profile_steps arguments");
+    return d->eng.profile_steps(nsteps, face_ms, elem_ms);
+}
+
+int esdg_advance(esdg_deviceclass* d, int nsteps, double T, double* t_out, int* steps_out) {
+    ESDG_GUARD(d);
+    if (nsteps < 0) return d->eng.fail(ESDG_E_ARG, "nsteps < 0");
+    if (!d->eng.graph) {
+        if (d->eng.gStages <= 0) return d->eng.fail(ESDG_E_ARG, "esdg_advance needs a previous esdg_dg_timeloop call");
+        int r = d->eng.capture_step_graph();
+        if (r) return r;
+    }
+    return d->eng.advance(nsteps, T, t_out, steps_out);
+}
+
+// ---------------------------------------------------------------------------
+// Set-up
+// ---------------------------------------------------------------------------
+int esdg_basis(int N, int FluxDifferencing, double* xGL, double* wGL, double* xG, double* wG, double* D, double* D0,
+               double* Dstrong, double* Dhat, double* VdmInv) {
+    if (N < 1 || N > 15) return ESDG_E_ARG;
+    esdg::Basis B;
+    esdg::build_basis(N, FluxDifferencing, &B);
+    const int n = N + 1;
+    auto cp = [](double* dst, const std::vector<double>& v) { if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double)); };
+    cp(xGL, B.xGL); cp(wGL, B.wGL); cp(xG, B.xG); cp(wG, B.wG);
+    cp(D, B.D); cp(D0, B.D0); cp(Dstrong, B.Dstrong); cp(Dhat, B.Dhat); cp(VdmInv, B.VdmInv);
+    (void)n;
+    return ESDG_OK;
+}
+
+int esdg_mesh_cartesian(int N, double xL, double xR, double yL, double yR, int NX, int NY, int periodic_rows,
+                        int periodic_cols, esdg_mesh** out) {
+    if (!out || N < 1 || N > 15 || NX < 1 || NY < 1) return ESDG_E_ARG;
+    if ((periodic_rows && NY < 2) || (periodic_cols && NX < 2)) return ESDG_E_ARG;
+    esdg_mesh* m = new (std::nothrow) esdg_mesh(N);
+    if (!m) return ESDG_E_NOMEM;
+    try {
+        m->m.generate_cartesian(xL, xR, yL, yR, NX, NY, periodic_rows != 0, periodic_cols != 0);
+    } catch (const std::exception& ex) {
+        esdg::g_create_error = ex.what();
+        delete m;
+        return ESDG_E_ARG;
+    }
+    *out = m;
+    return ESDG_OK;
+}
+
+int esdg_mesh_mapped(int N, double xL, double xR, double yL, double yR, int NX, int NY, double amp, int m_order,
+                     unsigned rotate_seed, esdg_mesh** out) {
+    if (!out || N < 1 || N > 15 || NX < 1 || NY < 1 || m_order < 1 || m_order > 32) return ESDG_E_ARG;
+    esdg_mesh* m = new (std::nothrow) esdg_mesh(N);
+    if (!m) return ESDG_E_NOMEM;
+    try {
+        m->m.generate_mapped(xL, xR, yL, yR, NX, NY, amp, m_order, rotate_seed);
+    } catch (const std::exception& ex) {
+        esdg::g_create_error = ex.what();
+        delete m;
+        return ESDG_E_ARG;
+    }
+    *out = m;
+    return ESDG_OK;
+}
+
+int esdg_mesh_read_ism2(int N, const char* path, int read_bottom, int convert_km, esdg_mesh** out) {
+    if (!out || !path || N < 1 || N > 15) return ESDG_E_ARG;
+    esdg_mesh* m = new (std::nothrow) esdg_mesh(N);
+    if (!m) return ESDG_E_NOMEM;
+    try {
+        m->m.read_ism2(path, read_bottom != 0, convert_km != 0);
+    } catch (const std::exception& ex) {
+        esdg::g_create_error = ex.what();
+        delete m;
+        return ESDG_E_IO;
+    }
+    *out = m;
+    return ESDG_OK;
+}
+
+int esdg_mesh_write_ism2(const esdg_mesh* m, const char* path) {
+    if (!m || !path) return ESDG_E_ARG;
+    try {
+        m->m.write_ism2(path);
+    } catch (const std::exception& ex) {
+        esdg::g_create_error = ex.what();
+        return ESDG_E_IO;
+    }
+    return ESDG_OK;
+}
+
+int esdg_mesh_sizes(const esdg_mesh* m, int* K, int* F) {
+    if (!m) return ESDG_E_ARG;
+    if (K) *K = m->m.K;
+    if (F) *F = m->m.F;
+    return ESDG_OK;
+}
+
+int esdg_mesh_pack(const esdg_mesh* m, double* x, double* y, double* x_xi, double* x_eta, double* y_xi,
+                   double* y_eta, double* Jinv, double* nx, double* ny, double* scal, double* b, int* EdgeData,
+                   int* EdgeReversed, int* ElemToEdge, int* ElemEdgeMasterSlave, int* ElemEdgeOrientation) {
+    if (!m) return ESDG_E_ARG;
+    esdg::PackedMesh P;
+    m->m.pack(&P);
+    auto cpd = [](double* dst, const std::vector<double>& v) { if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double)); };
+    auto cpi = [](int* dst, const std::vector<int>& v) { if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(int)); };
+    cpd(x, P.x); cpd(y, P.y); cpd(x_xi, P.xXi); cpd(x_eta, P.xEta); cpd(y_xi, P.yXi); cpd(y_eta, P.yEta);
+    cpd(Jinv, P.Jinv); cpd(nx, P.nx); cpd(ny, P.ny); cpd(scal, P.scal); cpd(b, P.b);
+    cpi(EdgeData, P.EdgeData); cpi(EdgeReversed, P.EdgeReversed); cpi(ElemToEdge, P.ElemToEdge);
+    cpi(ElemEdgeMasterSlave, P.MasterSlave); cpi(ElemEdgeOrientation, P.Orientation);
+    return ESDG_OK;
+}
+
+void esdg_mesh_free(esdg_mesh* m) { delete m; }
+
+int esdg_bottom_derivatives(int K, int N, const double* D0, const double* b, const double* y_eta, const double* y_xi,
+                            const double* x_eta, const double* x_xi, const double* Jinv, double* Bx, double* By) {
+    if (K <= 0 || N < 1 || !D0 || !b || !y_eta || !y_xi || !x_eta || !x_xi || !Jinv || !Bx || !By) return ESDG_E_ARG;
+    esdg::bottom_derivatives(K, N + 1, D0, b, y_eta, y_xi, x_eta, x_xi, Jinv, Bx, By);
+    return ESDG_OK;
+}
+
+int esdg_element_sizes(int K, int N, const double* wGL, const double* Jinv, double* EleSizes, double* minEleSize) {
+    if (K <= 0 || N < 1 || !wGL || !Jinv || !EleSizes || !minEleSize) return ESDG_E_ARG;
+    *minEleSize = esdg::element_sizes(K, N + 1, wGL, Jinv, EleSizes);
+    return ESDG_OK;
+}
+
+int esdg_rk_coefficients(int order, int ssp, double* A, double* B, double* C, int* stages) {
+    if (!A || !B || !C || !stages) return ESDG_E_ARG;
+    const int s = esdg::rk_coefficients(order, ssp, A, B, C);
+    if (s == 0) return ESDG_E_UNSUPPORTED;
+    *stages = s;
+    return ESDG_OK;
+}
+
+int esdg_diagnostics(int K, int N, const double* wGL, const double* Jinv, const double* q, const double* qref,
+                     const double* b, double g, double* L2, double* Linf, double* mass, double* entropy) {
+    if (K <= 0 || N < 1 || !wGL || !Jinv || !q) return ESDG_E_ARG;
+    esdg::diagnostics(K, N + 1, wGL, Jinv, q, qref, b, g, L2, Linf, mass, entropy);
+    return ESDG_OK;
+}
+
+}  // extern "C"

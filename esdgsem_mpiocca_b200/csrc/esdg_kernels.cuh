@@ -1,0 +1,734 @@
+// Per-stage kernels of the ES-DGSEM engine (sm_100a, FP64).
+//
+// One RK stage of the plain path is two launches:
+//   face_flux  : one thread per face node gathers the two traces straight
+//                from q (wall ghost on boundary faces), evaluates the ES
+//                Riemann flux once and writes the scaled flux F*[F][3][ngl];
+//   element    : NE elements per block staged in shared memory; flux-
+//                differencing volume integral, lifting of the four face
+//                fluxes, low-storage (or SSP) RK update and, on the last
+//                stage, the element wave-speed maximum for the next dt.
+// With artificial viscosity (BR1 gradient + viscous terms) a stage is four
+// launches: face_flux (+ gradient face flux), element_av1 (inviscid Qt,
+// shock sensor, lifted gradient), face_visc, element_av2 (viscous volume and
+// lift + RK update).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "esdg_physics.cuh"
+
+namespace esdg {
+
+enum : int { ST_OK = 0, ST_NONFINITE = 1 };
+
+// Per-instance time-stepping state, resident in device memory so that a
+// whole step runs without a host round trip (and can be graph-captured).
+struct DevState {
+    double t, dt, T, minEle, CFL, DFL;
+    unsigned long long lam_key, visc_key;
+    int steps, max_steps, done, status;
+};
+
+struct FaceArgs {
+    int F;
+    const int4* __restrict__ ftab;  // (elemL, elemR or -1, sideL | sideR<<2 | sameOrient<<4, 0)
+    const double* __restrict__ q;
+    const double* __restrict__ nx;
+    const double* __restrict__ ny;
+    const double* __restrict__ scal;
+    const double* __restrict__ bL;
+    const double* __restrict__ bR;
+    double* __restrict__ SP;   // [F][3][ngl]
+    double* __restrict__ SGX;  // [F][2][ngl] (AV only)
+    double* __restrict__ SGY;
+    const int* __restrict__ elem_inst;
+    const DevState* __restrict__ st;
+    PhysConst c;
+};
+
+struct ElemArgs {
+    int K;
+    const double* __restrict__ Jinv;
+    const double* __restrict__ Yxi;
+    const double* __restrict__ Yeta;
+    const double* __restrict__ Xxi;
+    const double* __restrict__ Xeta;
+    const double* __restrict__ Bx;
+    const double* __restrict__ By;
+    const double* __restrict__ B;
+    const double* __restrict__ D;       // flux-differencing matrix [ngl][ngl]
+    const double* __restrict__ Dhat;    // BR1 gradient matrix
+    const double* __restrict__ Dstrong; // viscous volume matrix
+    const double* __restrict__ Vinv;    // modal transform
+    const double* __restrict__ SP;      // face fluxes [F][3][ngl]
+    const double* __restrict__ SGX;     // gradient face fluxes [F][2][ngl]
+    const double* __restrict__ SGY;
+    const double* __restrict__ SPV;     // viscous face fluxes [F][2][ngl]
+    const int4* __restrict__ side;      // per element side: (face, masterSlave, orientation, 0)
+    double* q;
+    double* __restrict__ gRK;
+    double* __restrict__ Qt;
+    const double* __restrict__ Qtmp;
+    double* __restrict__ GX;            // [K][2][ngl][ngl]
+    double* __restrict__ GY;
+    double* __restrict__ VP;            // [K]
+    const int* __restrict__ elem_inst;
+    DevState* st;
+    double rkA, rkB, rkC;
+    int mode;        // 0: LS-RK update, 1: SSP update, 2: write Qt only
+    int lam;         // 1: element wave speed max into st[inst].lam_key after the update
+    int shock;       // AV: recompute the shock sensor into VP
+    PhysConst c;
+};
+
+__device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return elem_inst ? elem_inst[e] : 0; }
+
+// ---------------------------------------------------------------------------
+// Face kernel.
+// ---------------------------------------------------------------------------
+template <int NGL, int NUMFLUX, bool AV>
+__global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long)a.F * NGL) return;
+    const int f = (int)(gid / NGL), i = (int)(gid % NGL);
+    constexpr int N2 = NGL * NGL;
+    const int4 t = a.ftab[f];
+    const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
+    if (a.st[inst_of(a.elem_inst, eL)].done) return;
+    const int ir = same ? i : NGL - 1 - i;
+    const long ex = (long)f * NGL + i;
+    const double nx = a.nx[ex], ny = a.ny[ex];
+    const double* qe = a.q + (long)eL * 3 * N2;
+    const int oL = trace_offset(sL, i, NGL);
+    const double hL = qe[oL], huL = qe[oL + N2], hvL = qe[oL + 2 * N2];
+    double hR, huR, hvR;      // right state at master node i (flux)
+    double ghR, ghuR, ghvR;   // right state at node i in the right element's order (gradient)
+    if (eR >= 0) {
+        const double* qr = a.q + (long)eR * 3 * N2;
+        const int o = trace_offset(sR, ir, NGL);
+        hR = qr[o]; huR = qr[o + N2]; hvR = qr[o + 2 * N2];
+        if (AV) {
+            const int o2 = trace_offset(sR, i, NGL);
+            ghR = qr[o2]; ghuR = qr[o2 + N2]; ghvR = qr[o2 + 2 * N2];
+        }
+    } else {
+        // The reference stores the ghost of every face node in order and reads
+        // it back at node ir (okl/GatherEdgeData/SolidWalls.okl:150-173).
+        const long exr = (long)f * NGL + ir;
+        const int o = trace_offset(sL, ir, NGL);
+        wall_ghost(a.nx[exr], a.ny[exr], qe[o], qe[o + N2], qe[o + 2 * N2], hR, huR, hvR);
+        if (AV) { ghR = hL; ghuR = huL; ghvR = hvL; }
+    }
+    double N0, N1, N2f;
+    es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, a.bL[ex], a.bR[(long)f * NGL + ir], N0, N1, N2f);
+    const double s = a.scal[ex];
+    double* sp = a.SP + (long)f * 3 * NGL + i;
+    sp[0] = s * a.c.geomFace * N0;
+    sp[NGL] = s * a.c.geomFace * N1;
+    sp[2 * NGL] = s * a.c.geomFace * N2f;
+    if (AV) {
+        // okl/BR1_Gradient/calcNumFluxesGradient.okl:16-135 (the right trace
+        // is taken in the right element's own order, as there).
+        const double tol = a.c.PosPresTOL;
+        const double iL = (hL > tol) ? 1.0 / hL : 0.0;
+        const double iR = (ghR > tol) ? 1.0 / ghR : 0.0;
+        const double uL = huL * iL, uR = ghuR * iR, vL = hvL * iL, vR = ghvR * iR;
+        double* gx = a.SGX + (long)f * 2 * NGL + i;
+        double* gy = a.SGY + (long)f * 2 * NGL + i;
+        gx[0] = nx * s * a.c.geomFace * 0.5 * (uL + uR);
+        gx[NGL] = nx * s * a.c.geomFace * 0.5 * (vL + vR);
+        gy[0] = ny * s * a.c.geomFace * 0.5 * (uL + uR);
+        gy[NGL] = ny * s * a.c.geomFace * 0.5 * (vL + vR);
+    }
+}
+
+// Viscous face flux from the lifted gradients of both elements
+// (okl/BR1_Gradient/CollectEdgeDataGradient.okl:17-194 and
+// okl/ViscoseParts/calcNumFluxesViscose.okl:17-107); zero on walls.
+template <int NGL>
+__global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict__ ftab, const double* __restrict__ nxa,
+                                                   const double* __restrict__ nya, const double* __restrict__ scal,
+                                                   const double* __restrict__ GX, const double* __restrict__ GY,
+                                                   const double* __restrict__ VP, double* __restrict__ SPV,
+                                                   const int* __restrict__ elem_inst, const DevState* __restrict__ st,
+                                                   double geomFace) {
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long)F * NGL) return;
+    constexpr int N2 = NGL * NGL;
+    const int f = (int)(gid / NGL), i = (int)(gid % NGL);
+    const int4 t = ftab[f];
+    const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
+    if (st[inst_of(elem_inst, eL)].done) return;
+    const long ex = (long)f * NGL + i;
+    double N0 = 0.0, N1 = 0.0;
+    if (eR >= 0) {
+        const int inc = same ? i : NGL - 1 - i;
+        const long oL = (long)eL * 2 * N2 + trace_offset(sL, i, NGL);
+        const long oR = (long)eR * 2 * N2 + trace_offset(sR, inc, NGL);
+        const double nx = nxa[ex], ny = nya[ex];
+        const double f2L = nx * GX[oL] + ny * GY[oL], f2R = nx * GX[oR] + ny * GY[oR];
+        const double f3L = nx * GX[oL + N2] + ny * GY[oL + N2];
+        const double f3R = nx * GX[oR + N2] + ny * GY[oR + N2];
+        const double vm = fmax(VP[eL], VP[eR]);
+        N0 = 0.5 * vm * (f2L + f2R);
+        N1 = 0.5 * vm * (f3L + f3R);
+    }
+    const double s = scal[ex];
+    SPV[(long)f * 2 * NGL + i] = -s * geomFace * N0;
+    SPV[(long)f * 2 * NGL + NGL + i] = -s * geomFace * N1;
+}
+
+// ---------------------------------------------------------------------------
+// Element kernels.
+// ---------------------------------------------------------------------------
+template <int NGL>
+struct ElemShape {
+    static constexpr int N2 = NGL * NGL;
+    static constexpr int NE = (256 / N2) > 0 ? (256 / N2) : 1;  // elements per block
+    static constexpr int THREADS = NE * N2;
+};
+
+// Wave-speed maximum of the block's elements, folded into the owning
+// instance's key (okl/DG/FindLambdaMax.okl:17-100 per node; the reduction
+// is a max, so its order does not matter).
+template <int NGL, int NE>
+__device__ __forceinline__ void block_lambda(double lam, bool valid, int el, int nd, int e0, int K,
+                                             const int* elem_inst, DevState* st, double* sred) {
+    constexpr int N2 = NGL * NGL;
+    __syncthreads();
+    sred[el * N2 + nd] = valid ? lam : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int cur = -1;
+        double m = 0.0;
+        for (int k = 0; k < NE; ++k) {
+            const int e = e0 + k;
+            if (e >= K) break;
+            const int ins = inst_of(elem_inst, e);
+            double le = 0.0;
+            for (int p = 0; p < N2; ++p) {
+                const double v = sred[k * N2 + p];
+                le = (isnan(v) || v > le) ? v : le;
+            }
+            if (ins != cur) {
+                if (cur >= 0) atomicMax(&st[cur].lam_key, dbl_key(m));
+                cur = ins;
+                m = le;
+            } else {
+                m = (isnan(le) || le > m) ? le : m;
+            }
+        }
+        if (cur >= 0) atomicMax(&st[cur].lam_key, dbl_key(m));
+    }
+}
+
+__device__ __forceinline__ double node_lambda(const PhysConst& c, double h, double hu, double hv) {
+    const double inv = (h > c.PosPresTOL) ? 1.0 / h : 0.0;
+    const double cc = sqrt(c.g * h);
+    return cc + fmax(fabs(hu * inv), fabs(hv * inv));
+}
+
+// Flux-differencing volume term + surface lift (+ RK update).
+// okl/DG/VolumeKernelFluxDiffV99.okl:60-218, okl/DG/SurfaceKernel.okl:17-142,
+// okl/RungeKutta/rkLS.okl:17-89 + UpdateKernelLS.okl:17-78 (mode 0),
+// okl/RungeKutta/UpdateKernelSSP_V1.okl:17-98 (mode 1).
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sD[N2];
+    __shared__ double sh[NE * N2], shu[NE * N2], shv[NE * N2], si[NE * N2];
+    __shared__ double sYe[NE * N2], sYx[NE * N2], sXe[NE * N2], sXx[NE * N2];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int e0 = blockIdx.x * NE;
+    const int e = e0 + el;
+    const bool inb = e < a.K;
+    const int ins = inb ? inst_of(a.elem_inst, e) : 0;
+    const bool active = inb && !a.st[ins].done;
+    if (tid < N2) sD[tid] = a.D[tid];
+    const long xid = (long)e * N2 + nd, qid = (long)e * 3 * N2 + nd;
+    double h = 0, hu = 0, hv = 0;
+    const int s = el * N2 + nd;
+    if (active) {
+        h = a.q[qid]; hu = a.q[qid + N2]; hv = a.q[qid + 2 * N2];
+        sh[s] = h; shu[s] = hu; shv[s] = hv;
+        si[s] = (h > 0) ? 1.0 / h : 0.0;
+        sYe[s] = a.Yeta[xid]; sYx[s] = a.Yxi[xid]; sXe[s] = a.Xeta[xid]; sXx[s] = a.Xxi[xid];
+    }
+    __syncthreads();
+    double lam = 0.0;
+    if (active) {
+        const int xi = nd % NGL, eta = nd / NGL;
+        const int rb = el * N2 + eta * NGL;  // row base (same eta)
+        const int cb = el * N2 + xi;         // column base (same xi)
+        const double ih = si[s], ye = sYe[s], yx = sYx[s], xe = sXe[s], xx = sXx[s];
+        const double fg = a.c.fourth_g, hg = a.c.half_g;
+        double d1 = 0.0, d2 = 0.0, d3 = 0.0;
+#pragma unroll
+        for (int l = 0; l < NGL; ++l) {
+            const int p = rb + l;
+            const double dl = sD[xi * NGL + l];
+            double f1, f2, f3;
+            two_point_xi(fg, hg, h, hu, hv, ih, sh[p], shu[p], shv[p], si[p], ye, sYe[p], xe, sXe[p], f1, f2, f3);
+            d1 += dl * f1; d2 += dl * f2; d3 += dl * f3;
+        }
+#pragma unroll
+        for (int l = 0; l < NGL; ++l) {
+            const int p = cb + l * NGL;
+            const double dl = sD[eta * NGL + l];
+            double g1, g2, g3;
+            two_point_eta(fg, hg, h, hu, hv, ih, sh[p], shu[p], shv[p], si[p], yx, sYx[p], xx, sXx[p], g1, g2, g3);
+            d1 += dl * g1; d2 += dl * g2; d3 += dl * g3;
+        }
+        const double J = a.Jinv[xid];
+        double r0 = -J * d1;
+        double r1 = -J * d2 - a.c.g * h * a.Bx[xid];
+        double r2 = -J * d3 - a.c.g * h * a.By[xid];
+        // lift: sides 0/2 first, then 1/3
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            int side = -1, j = 0;
+            if (pass == 0) {
+                if (eta == 0) { side = 0; j = xi; }
+                else if (eta == NGL - 1) { side = 2; j = xi; }
+            } else {
+                if (xi == NGL - 1) { side = 1; j = eta; }
+                else if (xi == 0) { side = 3; j = eta; }
+            }
+            if (side >= 0) {
+                const int4 sd = a.side[(long)e * 4 + side];
+                const int inc = sd.z ? j : NGL - 1 - j;
+                const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
+                const int ms = sd.y;
+                const double db = 0.0;
+                r0 += -ms * fp[0] * J;
+                r1 += -ms * J * fp[NGL] + J * db;
+                r2 += -ms * J * fp[2 * NGL] + J * db;
+            }
+        }
+        if (a.mode == 2) {
+            a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
+        } else {
+            const double dt = a.st[ins].dt;
+            double q0, q1, q2;
+            if (a.mode == 0) {
+                const double g0 = a.rkA * a.gRK[qid] + r0;
+                const double g1 = a.rkA * a.gRK[qid + N2] + r1;
+                const double g2 = a.rkA * a.gRK[qid + 2 * N2] + r2;
+                a.gRK[qid] = g0; a.gRK[qid + N2] = g1; a.gRK[qid + 2 * N2] = g2;
+                q0 = h + a.rkC * dt * g0;
+                q1 = hu + a.rkC * dt * g1;
+                q2 = hv + a.rkC * dt * g2;
+            } else {
+                q0 = a.rkA * a.Qtmp[qid] + a.rkB * h + a.rkC * dt * r0;
+                q1 = a.rkA * a.Qtmp[qid + N2] + a.rkB * hu + a.rkC * dt * r1;
+                q2 = a.rkA * a.Qtmp[qid + 2 * N2] + a.rkB * hv + a.rkC * dt * r2;
+            }
+            a.q[qid] = q0; a.q[qid + N2] = q1; a.q[qid + 2 * N2] = q2;
+            if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
+        }
+    }
+    if (a.lam) block_lambda<NGL, NE>(lam, active, el, nd, e0, a.K, a.elem_inst, a.st, sh);
+}
+
+// Modal energy sensor of one element (okl/ShockCapturing/ShockCapturing.okl:17-234),
+// evaluated by one thread; m = (h+b) nodal values [eta][xi], V = VdmInv
+// row-major [mode][node]; w receives the modal coefficients [mode_xi][mode_eta].
+template <int NGL>
+__device__ double shock_sensor(const PhysConst& c, const double* m, const double* V, double* w) {
+    // s_Q1modal[i][j] in the reference holds node (xi=i, eta=j).
+    constexpr int N = NGL - 1;
+    double M1[NGL * NGL];
+    for (int i = 0; i < NGL; ++i)
+        for (int j = 0; j < NGL; ++j) {
+            double acc = 0.0;
+            for (int l = 0; l < NGL; ++l) acc += V[i * NGL + l] * m[j * NGL + l];
+            M1[i * NGL + j] = acc;
+        }
+    for (int i = 0; i < NGL; ++i)
+        for (int j = 0; j < NGL; ++j) {
+            double acc = 0.0;
+            for (int l = 0; l < NGL; ++l) acc += M1[i * NGL + l] * V[j * NGL + l];
+            w[i * NGL + j] = acc;
+        }
+    double z1 = 0, n1 = 0, z2 = 0, n2s = 0;
+    for (int i = 0; i < N; ++i) z1 += w[i * NGL + N] * w[i * NGL + N] + w[N * NGL + i] * w[N * NGL + i];
+    z1 += w[N * NGL + N] * w[N * NGL + N];
+    for (int i = 0; i < N - 1; ++i)
+        z2 += w[i * NGL + N - 1] * w[i * NGL + N - 1] + w[(N - 1) * NGL + i] * w[(N - 1) * NGL + i];
+    z2 += w[(N - 1) * NGL + N - 1] * w[(N - 1) * NGL + N - 1];
+    for (int i = 0; i < NGL; ++i)
+        for (int j = 0; j < NGL; ++j) n1 += w[i * NGL + j] * w[i * NGL + j];
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) n2s += w[i * NGL + j] * w[i * NGL + j];
+    const double t1 = (n1 < c.ZeroTOL) ? 0.0 : z1 / n1;
+    const double t2 = (n1 < c.ZeroTOL) ? 0.0 : z2 / n2s;
+    const double sig = log10((t1 < t2) ? t2 : t1);
+    if (c.sigmaMin >= sig) return 0.0;
+    if (c.sigmaMax >= sig) {
+        const double delta = 1.0 + sin(M_PI * (sig - 0.5 * (c.sigmaMax + c.sigmaMin)) / (c.sigmaMax - c.sigmaMin));
+        return c.eps0 * 0.5 * delta;
+    }
+    return c.eps0;
+}
+
+// Shock sensor for every element and the per-instance maximum viscosity
+// (src/deviceclass.cpp:914-924).  One element per warp.
+template <int NGL>
+__global__ void __launch_bounds__(256) k_shock(int K, const double* __restrict__ q, const double* __restrict__ B,
+                                               const double* __restrict__ Vinv, double* __restrict__ VP,
+                                               const int* __restrict__ elem_inst, DevState* st, PhysConst c) {
+    constexpr int N2 = NGL * NGL;
+    __shared__ double sm[8][N2], sw[8][N2], sV[N2];
+    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (threadIdx.x < N2) sV[threadIdx.x] = Vinv[threadIdx.x];
+    __syncthreads();
+    const int e = blockIdx.x * 8 + w;
+    if (e >= K) return;
+    const int ins = inst_of(elem_inst, e);
+    if (st[ins].done) return;
+    for (int p = lane; p < N2; p += 32) sm[w][p] = B[(long)e * N2 + p] + q[(long)e * 3 * N2 + p];
+    __syncwarp();
+    if (lane == 0) {
+        const double v = shock_sensor<NGL>(c, sm[w], sV, sw[w]);
+        VP[e] = v;
+        atomicMax(&st[ins].visc_key, dbl_key(v));
+    }
+}
+
+// Inviscid volume + lift written to Qt, shock sensor (stages > 0) and the
+// lifted, h-scaled BR1 gradient of the velocities.
+// okl/BR1_Gradient/calcGradient.okl:18-156, SurfaceKernelGradient.okl:16-150,
+// scaleGradient.okl:17-60.
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av1(ElemArgs a) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sD[N2], sDh[N2], sV[N2];
+    __shared__ double sh[NE * N2], shu[NE * N2], shv[NE * N2], si[NE * N2];
+    __shared__ double sYe[NE * N2], sYx[NE * N2], sXe[NE * N2], sXx[NE * N2];
+    __shared__ double su[NE * N2], sv[NE * N2];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int e0 = blockIdx.x * NE;
+    const int e = e0 + el;
+    const bool inb = e < a.K;
+    const int ins = inb ? inst_of(a.elem_inst, e) : 0;
+    const bool active = inb && !a.st[ins].done;
+    if (tid < N2) {
+        sD[tid] = a.D[tid];
+        sDh[tid] = a.Dhat[tid];
+        sV[tid] = a.Vinv[tid];
+    }
+    const long xid = (long)e * N2 + nd, qid = (long)e * 3 * N2 + nd;
+    const int s = el * N2 + nd;
+    double h = 0, hu = 0, hv = 0;
+    if (active) {
+        h = a.q[qid]; hu = a.q[qid + N2]; hv = a.q[qid + 2 * N2];
+        sh[s] = h; shu[s] = hu; shv[s] = hv;
+        si[s] = (h > 0) ? 1.0 / h : 0.0;
+        const double iv = (h > a.c.PosPresTOL) ? 1.0 / h : 0.0;
+        su[s] = hu * iv; sv[s] = hv * iv;
+        sYe[s] = a.Yeta[xid]; sYx[s] = a.Yxi[xid]; sXe[s] = a.Xeta[xid]; sXx[s] = a.Xxi[xid];
+    }
+    __syncthreads();
+    if (!active) return;  // no further block-wide synchronisation below
+    const int xi = nd % NGL, eta = nd / NGL;
+    const double J = a.Jinv[xid];
+    {
+        const int rb = el * N2 + eta * NGL, cb = el * N2 + xi;
+        const double ih = si[s], ye = sYe[s], yx = sYx[s], xe = sXe[s], xx = sXx[s];
+        const double fg = a.c.fourth_g, hg = a.c.half_g;
+        double d1 = 0.0, d2 = 0.0, d3 = 0.0;
+#pragma unroll
+        for (int l = 0; l < NGL; ++l) {
+            const int p = rb + l;
+            const double dl = sD[xi * NGL + l];
+            double f1, f2, f3;
+            two_point_xi(fg, hg, h, hu, hv, ih, sh[p], shu[p], shv[p], si[p], ye, sYe[p], xe, sXe[p], f1, f2, f3);
+            d1 += dl * f1; d2 += dl * f2; d3 += dl * f3;
+        }
+#pragma unroll
+        for (int l = 0; l < NGL; ++l) {
+            const int p = cb + l * NGL;
+            const double dl = sD[eta * NGL + l];
+            double g1, g2, g3;
+            two_point_eta(fg, hg, h, hu, hv, ih, sh[p], shu[p], shv[p], si[p], yx, sYx[p], xx, sXx[p], g1, g2, g3);
+            d1 += dl * g1; d2 += dl * g2; d3 += dl * g3;
+        }
+        double r0 = -J * d1;
+        double r1 = -J * d2 - a.c.g * h * a.Bx[xid];
+        double r2 = -J * d3 - a.c.g * h * a.By[xid];
+        double gx0 = 0, gx1 = 0, gy0 = 0, gy1 = 0;
+        {
+            // calcGradient: u_xi = sum_l Dhat[xi][l] u(l,eta), u_eta = sum_l Dhat[eta][l] u(xi,l)
+            double uxi = 0, ueta = 0, vxi = 0, veta = 0;
+#pragma unroll
+            for (int l = 0; l < NGL; ++l) {
+                uxi += sDh[xi * NGL + l] * su[rb + l];
+                ueta += sDh[eta * NGL + l] * su[cb + l * NGL];
+                vxi += sDh[xi * NGL + l] * sv[rb + l];
+                veta += sDh[eta * NGL + l] * sv[cb + l * NGL];
+            }
+            const double ux = ye * uxi - yx * ueta, vx = ye * vxi - yx * veta;
+            const double uy = -xe * uxi + xx * ueta, vy = -xe * vxi + xx * veta;
+            gx0 = J * ux; gx1 = J * vx; gy0 = J * uy; gy1 = J * vy;
+        }
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            int side = -1, j = 0;
+            if (pass == 0) {
+                if (eta == 0) { side = 0; j = xi; }
+                else if (eta == NGL - 1) { side = 2; j = xi; }
+            } else {
+                if (xi == NGL - 1) { side = 1; j = eta; }
+                else if (xi == 0) { side = 3; j = eta; }
+            }
+            if (side >= 0) {
+                const int4 sd = a.side[(long)e * 4 + side];
+                const int inc = sd.z ? j : NGL - 1 - j;
+                const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
+                const int ms = sd.y;
+                const double db = 0.0;
+                r0 += -ms * fp[0] * J;
+                r1 += -ms * J * fp[NGL] + J * db;
+                r2 += -ms * J * fp[2 * NGL] + J * db;
+                const double* ux = a.SGX + (long)sd.x * 2 * NGL + inc;
+                const double* uy = a.SGY + (long)sd.x * 2 * NGL + inc;
+                if (pass == 0) gx0 += ms * ux[0] * J;
+                else gx0 += ms * J * ux[0];
+                gx1 += ms * J * ux[NGL];
+                gy0 += ms * J * uy[0];
+                gy1 += ms * J * uy[NGL];
+            }
+        }
+        a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
+        const long gid = (long)e * 2 * N2 + nd;
+        a.GX[gid] = h * gx0; a.GX[gid + N2] = h * gx1;
+        a.GY[gid] = h * gy0; a.GY[gid + N2] = h * gy1;
+    }
+    if (a.shock && nd == 0) {
+        // (h + b) of this element; sh is not written after the staging sync.
+        double m[N2], w[N2];
+        for (int p = 0; p < N2; ++p) m[p] = a.B[(long)e * N2 + p] + sh[el * N2 + p];
+        const double v = shock_sensor<NGL>(a.c, m, sV, w);
+        a.VP[e] = v;
+    }
+}
+
+// Viscous volume term + viscous lift added to Qt, then the RK update.
+// okl/ViscoseParts/VolumeKernelViscose.okl:17-150, SurfaceKernelVisc.okl:17-144.
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av2(ElemArgs a) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sDs[N2];
+    __shared__ double sF2[NE * N2], sF3[NE * N2], sG2[NE * N2], sG3[NE * N2];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int e0 = blockIdx.x * NE;
+    const int e = e0 + el;
+    const bool inb = e < a.K;
+    const int ins = inb ? inst_of(a.elem_inst, e) : 0;
+    const bool active = inb && !a.st[ins].done;
+    if (tid < N2) sDs[tid] = a.Dstrong[tid];
+    const long xid = (long)e * N2 + nd, qid = (long)e * 3 * N2 + nd, gid = (long)e * 2 * N2 + nd;
+    const int s = el * N2 + nd;
+    if (active) {
+        const double eps = a.VP[e];
+        const double F2 = eps * a.GX[gid], F3 = eps * a.GX[gid + N2];
+        const double G2 = eps * a.GY[gid], G3 = eps * a.GY[gid + N2];
+        const double ye = a.Yeta[xid], yx = a.Yxi[xid], xe = a.Xeta[xid], xx = a.Xxi[xid];
+        sF2[s] = ye * F2 - xe * G2;
+        sG2[s] = -yx * F2 + xx * G2;
+        sF3[s] = ye * F3 - xe * G3;
+        sG3[s] = -yx * F3 + xx * G3;
+    }
+    __syncthreads();
+    double lam = 0.0;
+    if (active) {
+        const int xi = nd % NGL, eta = nd / NGL;
+        const int rb = el * N2 + eta * NGL, cb = el * N2 + xi;
+        double d2 = 0, d3 = 0;
+#pragma unroll
+        for (int l = 0; l < NGL; ++l) {
+            d2 += sDs[xi * NGL + l] * sF2[rb + l];
+            d2 += sDs[eta * NGL + l] * sG2[cb + l * NGL];
+            d3 += sDs[xi * NGL + l] * sF3[rb + l];
+            d3 += sDs[eta * NGL + l] * sG3[cb + l * NGL];
+        }
+        const double J = a.Jinv[xid];
+        double r0 = a.Qt[qid], r1 = a.Qt[qid + N2], r2 = a.Qt[qid + 2 * N2];
+        r1 += J * d2;
+        r2 += J * d3;
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            int side = -1, j = 0;
+            if (pass == 0) {
+                if (eta == 0) { side = 0; j = xi; }
+                else if (eta == NGL - 1) { side = 2; j = xi; }
+            } else {
+                if (xi == NGL - 1) { side = 1; j = eta; }
+                else if (xi == 0) { side = 3; j = eta; }
+            }
+            if (side >= 0) {
+                const int4 sd = a.side[(long)e * 4 + side];
+                const int inc = sd.z ? j : NGL - 1 - j;
+                const double* fp = a.SPV + (long)sd.x * 2 * NGL + inc;
+                const int ms = sd.y;
+                r1 += -ms * J * fp[0];
+                r2 += -ms * J * fp[NGL];
+            }
+        }
+        const double h = a.q[qid], hu = a.q[qid + N2], hv = a.q[qid + 2 * N2];
+        if (a.mode == 2) {
+            a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
+        } else {
+            const double dt = a.st[ins].dt;
+            double q0, q1, q2;
+            if (a.mode == 0) {
+                const double g0 = a.rkA * a.gRK[qid] + r0;
+                const double g1 = a.rkA * a.gRK[qid + N2] + r1;
+                const double g2 = a.rkA * a.gRK[qid + 2 * N2] + r2;
+                a.gRK[qid] = g0; a.gRK[qid + N2] = g1; a.gRK[qid + 2 * N2] = g2;
+                q0 = h + a.rkC * dt * g0;
+                q1 = hu + a.rkC * dt * g1;
+                q2 = hv + a.rkC * dt * g2;
+            } else {
+                q0 = a.rkA * a.Qtmp[qid] + a.rkB * h + a.rkC * dt * r0;
+                q1 = a.rkA * a.Qtmp[qid + N2] + a.rkB * hu + a.rkC * dt * r1;
+                q2 = a.rkA * a.Qtmp[qid + 2 * N2] + a.rkB * hv + a.rkC * dt * r2;
+            }
+            a.q[qid] = q0; a.q[qid + N2] = q1; a.q[qid + 2 * N2] = q2;
+            if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
+        }
+    }
+    if (a.lam) block_lambda<NGL, NE>(lam, active, el, nd, e0, a.K, a.elem_inst, a.st, sF2);
+}
+
+// Positivity limiter (okl/Positivity/PosPres.okl:17-223), optionally with the
+// wave-speed maximum of the limited state.
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_pospres(int K, const double* __restrict__ EleSizes,
+                                                                   const double* __restrict__ GLw,
+                                                                   const double* __restrict__ Jinv, double* q,
+                                                                   const int* __restrict__ elem_inst, DevState* st,
+                                                                   int lam_flag, PhysConst c) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sH[NE * N2], sU[NE * N2], sVv[NE * N2], sJ[NE * N2];
+    __shared__ double sAvg[NE][4];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int e0 = blockIdx.x * NE;
+    const int e = e0 + el;
+    const bool inb = e < K;
+    const int ins = inb ? inst_of(elem_inst, e) : 0;
+    const bool active = inb && !st[ins].done;
+    const long qid = (long)e * 3 * N2 + nd;
+    const int s = el * N2 + nd;
+    if (active) {
+        sH[s] = q[qid]; sU[s] = q[qid + N2]; sVv[s] = q[qid + 2 * N2];
+        sJ[s] = Jinv[(long)e * N2 + nd];
+    }
+    __syncthreads();
+    if (active && nd == 0) {
+        double hmin = 0.0, ha = 0.0, hua = 0.0, hva = 0.0;
+        for (int l = 0; l < NGL; ++l)
+            for (int k = 0; k < NGL; ++k) {
+                const int p = el * N2 + k * NGL + l;
+                const double w = GLw[l] * GLw[k] / sJ[p];
+                ha += sH[p] * w;
+                hua += sU[p] * w;
+                hva += sVv[p] * w;
+                hmin = fmin(hmin, sH[p]);
+            }
+        const double es = EleSizes[e];
+        ha = ha / es;
+        if (fabs(ha) < c.ZeroTOL) ha = 0.0;
+        sAvg[el][0] = ha;
+        sAvg[el][1] = hua / es;
+        sAvg[el][2] = hva / es;
+        sAvg[el][3] = hmin;
+    }
+    __syncthreads();
+    double lam = 0.0;
+    if (active) {
+        const double ha = sAvg[el][0], hua = sAvg[el][1], hva = sAvg[el][2], hmin = sAvg[el][3];
+        const double theta = (ha == hmin) ? 1.0 : fmin(1.0, ha / (ha - hmin));
+        double h = sH[s], hu = sU[s], hv = sVv[s];
+        if (hmin < 0.0) {
+            double hn = 0.0, hun = 0.0, hvn = 0.0;
+            if (ha > 0.0) {
+                hn = fabs(theta * (h - ha) + ha);
+                if (hn > c.PosPresTOL) {
+                    hun = theta * (hu - hua) + hua;
+                    hvn = theta * (hv - hva) + hva;
+                }
+            }
+            if (ha < 0.0) { hn = -1.0 / 0.0; hun = 0.0; hvn = 0.0; }  // -inf marks a failed limiter
+            h = hn; hu = hun; hv = hvn;
+            q[qid] = h; q[qid + N2] = hu; q[qid + 2 * N2] = hv;
+        } else if (h < c.PosPresTOL) {
+            hu = 0.0; hv = 0.0;
+            q[qid + N2] = 0.0; q[qid + 2 * N2] = 0.0;
+        }
+        if (lam_flag) lam = node_lambda(c, h, hu, hv);
+    }
+    if (lam_flag) block_lambda<NGL, NE>(lam, active, el, nd, e0, K, elem_inst, st, sJ);
+}
+
+// Wave-speed maximum of q (start of the time loop).
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_lambda(int K, const double* __restrict__ q,
+                                                                  const int* __restrict__ elem_inst, DevState* st,
+                                                                  PhysConst c) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sred[NE * N2];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int e0 = blockIdx.x * NE;
+    const int e = e0 + el;
+    const bool inb = e < K;
+    double lam = 0.0;
+    if (inb) {
+        const long qid = (long)e * 3 * N2 + nd;
+        lam = node_lambda(c, q[qid], q[qid + N2], q[qid + 2 * N2]);
+    }
+    block_lambda<NGL, NE>(lam, inb, el, nd, e0, K, elem_inst, st, sred);
+}
+
+// Step bookkeeping per instance (src/deviceclass.cpp:897-930 and :1130):
+// dt from the CFL and viscous limits, done flag when t >= T or the step cap
+// is reached.
+__global__ void k_step_begin(int I, DevState* st, int ngl, int AV) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= I) return;
+    DevState& s = st[k];
+    if (s.done) return;
+    if (!(s.t < s.T) || (s.max_steps > 0 && s.steps >= s.max_steps)) { s.done = 1; return; }
+    const double lam = __longlong_as_double((long long)s.lam_key);
+    if (s.lam_key == ~0ull || !isfinite(lam)) { s.status = ST_NONFINITE; s.done = 1; return; }
+    const double dt_i = s.minEle / (double)ngl * s.CFL / lam;
+    double dt;
+    if (AV) {
+        const double vmax = __longlong_as_double((long long)s.visc_key);
+        const double dt_v = s.DFL / (pow((double)ngl, 2)) * pow(s.minEle, 2) / vmax;
+        dt = fmin(s.T - s.t, fmin(dt_i, dt_v));
+    } else {
+        dt = fmin(s.T - s.t, dt_i);
+    }
+    s.dt = dt;
+    s.lam_key = 0ull;
+    s.visc_key = 0ull;
+}
+
+__global__ void k_step_end(int I, DevState* st) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= I) return;
+    DevState& s = st[k];
+    if (s.done) return;
+    s.t += s.dt;
+    s.steps += 1;
+}
+
+}  // namespace esdg

@@ -1,0 +1,176 @@
+"""Python mirror of the reference's ``deviceclass`` (include/deviceclass.h:28-138)
+over the C ABI of libesdg_b200.so.  Method names, argument order and meaning
+follow the reference; errors raise ``EsdgError`` carrying the engine's
+status code and message (the reference aborts or throws instead).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import lib as _lib
+from .host import Problem, pd, pi
+
+E_ARG, E_UNSUPPORTED, E_CUDA, E_NONFINITE, E_IO, E_NOMEM = -1, -2, -3, -4, -5, -6
+
+
+class EsdgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class DeviceClass:
+    """One engine handle (one GPU, one mesh)."""
+
+    def __init__(self, rank: int = 0, device_id: int = -1):
+        self._L = _lib()
+        h = ctypes.c_void_p()
+        rc = self._L.esdg_deviceclass_create(rank, device_id, ctypes.byref(h))
+        if rc != 0:
+            raise EsdgError(rc, self._L.esdg_last_error(None).decode())
+        self.h = h
+        self._keep = []
+
+    def _ok(self, rc):
+        if rc != 0:
+            raise EsdgError(rc, self._L.esdg_last_error(self.h).decode())
+
+    # -- reference surface -------------------------------------------------
+    def initDeviceVariables(self, N, Nelem, Nfaces, rank, rkSSP, NEpad, NEsurfpad, Nedgepad, NAvgPad, ES, Testcase,
+                            epsilon_0, sigma_max, sigma_min, PosPresTOL, geomface, g_const, PositivityPreserving,
+                            ArtificialViscosity, DiscBottom, h_0, PartialDry, FrictionTerms, CalcArrivalTimes,
+                            CreateTimeSeries, CalcMaximumElevation):
+        self._ok(self._L.esdg_init_device_variables(
+            self.h, N, Nelem, Nfaces, rank, rkSSP, NEpad, NEsurfpad, Nedgepad, NAvgPad, ES, Testcase, epsilon_0,
+            sigma_max, sigma_min, PosPresTOL, geomface, g_const, PositivityPreserving, ArtificialViscosity,
+            DiscBottom, h_0, PartialDry, FrictionTerms, CalcArrivalTimes, CreateTimeSeries, CalcMaximumElevation))
+
+    def copyDeviceVariables(self, PositivityPreserving, Nelem, GLw, normalsX, normalsY, Scal, y_xi, y_eta, x_xi,
+                            x_eta, b, Bx, By, Dmat, Dstrong, Dhat, J, x_phy, y_phy, q, ElementSizes, gRK, Qt, VdmInv,
+                            ElemEdgeMasterSlave, ElemEdgeOrientation, ElemToEdge, EdgeData, EdgeReversed):
+        d = [_f64(a) for a in (GLw, normalsX, normalsY, Scal, y_xi, y_eta, x_xi, x_eta, b, Bx, By, Dmat, Dstrong,
+                               Dhat, J, x_phy, y_phy, q, ElementSizes, gRK, Qt, VdmInv)]
+        i = [_i32(a) for a in (ElemEdgeMasterSlave, ElemEdgeOrientation, ElemToEdge, EdgeData, EdgeReversed)]
+        self._ok(self._L.esdg_copy_device_variables(self.h, PositivityPreserving, Nelem, *[pd(a) for a in d],
+                                                    *[pi(a) for a in i]))
+
+    def buildDeviceKernels(self, KernelVersion, KernelVersionSTD, Testcase, FluxDifferencing, NumFlux, rkSSP,
+                           ArtificialViscosity, PositivityPreserving, DiscBottom):
+        self._ok(self._L.esdg_build_device_kernels(self.h, KernelVersion, KernelVersionSTD, Testcase,
+                                                   FluxDifferencing, NumFlux, rkSSP, ArtificialViscosity,
+                                                   PositivityPreserving, DiscBottom))
+
+    def DGtimeloop(self, Nelem, Nfaces, rkA, rkB, rkC, globalMinEleSize, CFL, DFL, T, Testcase, ArtificialViscosity,
+                   rkSSP, NumPlots, NumTimeChecks, g_const, PlotVar, EntropyPlot, PositivityPreserving, DiscBottom,
+                   max_steps=0):
+        A, B, C = _f64(rkA), _f64(rkB), _f64(rkC)
+        t = ctypes.c_double()
+        s = ctypes.c_int()
+        self._ok(self._L.esdg_dg_timeloop(self.h, Nelem, Nfaces, len(A), pd(A), pd(B), pd(C), globalMinEleSize, CFL,
+                                          DFL, T, Testcase, ArtificialViscosity, rkSSP, NumPlots, NumTimeChecks,
+                                          g_const, PlotVar, EntropyPlot, PositivityPreserving, DiscBottom, max_steps,
+                                          ctypes.byref(t), ctypes.byref(s)))
+        return t.value, s.value
+
+    def copy_q_to_host(self, q: np.ndarray):
+        assert q.dtype == np.float64 and q.flags.c_contiguous
+        self._ok(self._L.esdg_copy_q_to_host(self.h, pd(q)))
+        return q
+
+    def copy_q_from_host(self, q: np.ndarray):
+        q = _f64(q)
+        self._ok(self._L.esdg_copy_q_from_host(self.h, pd(q)))
+
+    def bytesAllocated(self) -> int:
+        return int(self._L.esdg_bytes_allocated(self.h))
+
+    def freeOccaVars(self, rkSSP=0, PositivityPreserving=0, ArtificialViscosity=0):
+        self._ok(self._L.esdg_free_occa_vars(self.h, rkSSP, PositivityPreserving, ArtificialViscosity))
+
+    # -- engine extras ------------------------------------------------------
+    def compute_rhs(self, K, ngl, AV=False):
+        Qt = np.zeros(K * 3 * ngl * ngl)
+        visc = np.zeros(K) if AV else None
+        self._ok(self._L.esdg_compute_rhs(self.h, pd(Qt), pd(visc)))
+        return (Qt, visc) if AV else Qt
+
+    def copy_visc_to_host(self, K):
+        v = np.zeros(K)
+        self._ok(self._L.esdg_copy_visc_to_host(self.h, pd(v)))
+        return v
+
+    def set_stream(self, stream_ptr: int | None):
+        self._ok(self._L.esdg_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def advance(self, nsteps: int, T: float):
+        t = ctypes.c_double()
+        s = ctypes.c_int()
+        self._ok(self._L.esdg_advance(self.h, nsteps, T, ctypes.byref(t), ctypes.byref(s)))
+        return t.value, s.value
+
+    def profile_steps(self, nsteps: int):
+        f = ctypes.c_double()
+        e = ctypes.c_double()
+        self._ok(self._L.esdg_profile_steps(self.h, nsteps, ctypes.byref(f), ctypes.byref(e)))
+        return f.value, e.value
+
+    def kernel_launches(self) -> int:
+        return int(self._L.esdg_kernel_launches(self.h))
+
+    def close(self):
+        if self.h is not None and self.h.value:
+            self._L.esdg_deviceclass_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """main.cpp:925-1051 for one Problem: init, copy, build, time loop."""
+
+    def __init__(self, prob: Problem, device_id: int = -1, q0=None):
+        self.prob = prob
+        p, m, bs = prob.params, prob.mesh, prob.basis
+        self.dc = DeviceClass(0, device_id)
+        self.dc.initDeviceVariables(p.N, m.K, m.F, 0, p.rkSSP, p.NEpad, p.NEsurfpad, p.Nedgepad, p.NavgPad, p.ES,
+                                    p.Testcase, p.epsilon_0, p.sigma_max, p.sigma_min, p.PosPresTOL, bs.geomface,
+                                    p.g_const, p.PositivityPreserving, p.ArtificialViscosity, p.DiscBottom, 0.0, 0, 0,
+                                    0, 0, 0)
+        zeros = np.zeros_like(prob.q0)
+        self.dc.copyDeviceVariables(p.PositivityPreserving, m.K, bs.wGL, m.nx, m.ny, m.scal, m.y_xi, m.y_eta, m.x_xi,
+                                    m.x_eta, prob.b, prob.Bx, prob.By, bs.D, bs.Dstrong, bs.Dhat, m.Jinv, m.x, m.y,
+                                    prob.q0 if q0 is None else q0, prob.EleSizes, zeros, zeros, bs.VdmInv,
+                                    m.MasterSlave, m.Orientation, m.ElemToEdge, m.EdgeData, m.EdgeReversed)
+        self.dc.buildDeviceKernels(99, 99, p.Testcase, p.FluxDifferencing, p.NumFlux, p.rkSSP, p.ArtificialViscosity,
+                                   p.PositivityPreserving, p.DiscBottom)
+
+    def run(self, T=None, max_steps=None):
+        p, prob = self.prob.params, self.prob
+        T = p.T if T is None else T
+        ms = p.MaxSteps if max_steps is None else max_steps
+        return self.dc.DGtimeloop(prob.K, prob.F, prob.rkA, prob.rkB, prob.rkC, prob.minEleSize, p.CFL, p.DFL, T,
+                                  p.Testcase, p.ArtificialViscosity, p.rkSSP, 0, 0, p.g_const, 0, 0,
+                                  p.PositivityPreserving, p.DiscBottom, ms)
+
+    def q(self):
+        return self.dc.copy_q_to_host(np.zeros_like(self.prob.q0))
+
+    def rhs(self):
+        return self.dc.compute_rhs(self.prob.K, self.prob.ngl, bool(self.prob.params.ArtificialViscosity))
+
+    def close(self):
+        self.dc.close()

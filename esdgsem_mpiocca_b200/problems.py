@@ -1,0 +1,88 @@
+"""Seeded synthetic problems with the shapes of the benchmark configurations.
+
+The reference publishes no dataset; each configuration is generated here from
+its description (mesh, bathymetry, initial state, solver switches), seeded so
+that every run and every test sees the same numbers.
+
+  periodic_bump   N=3, 16x16 periodic Cartesian on [0,2]^2, b=0.1 sin(pi x)cos(pi y),
+                  h = 1-b+0.05 exp(-50 r^2)                      (100 LS-RK4 steps, CFL 0.4)
+  curved_lake     N=4, curved 512x512 on [0,1]^2 (x+0.03 sin sin), walls, 8 seeded
+                  Gaussian bumps, lake at rest + seeded ripple   (1000 steps)
+  dam_break       N=4, curved 256x256, b=0, circular dam of radius U[0.2,0.35], AV on
+  tsunami_member  N=3, one ensemble member on a 2000 km square with a shelf,
+                  seamounts and an Okada-type uplift (see ensemble.py)
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .host import Params, Problem, make_problem, mesh_cartesian, mesh_mapped
+
+
+def _state(h, hu=None, hv=None, K=None, n2=None):
+    """Pack nodal h, hu, hv [K*n2] into q [K][3][n2]."""
+    q = np.zeros((K, 3, n2))
+    q[:, 0, :] = h.reshape(K, n2)
+    if hu is not None:
+        q[:, 1, :] = hu.reshape(K, n2)
+    if hv is not None:
+        q[:, 2, :] = hv.reshape(K, n2)
+    return q.reshape(-1)
+
+
+def periodic_bump(N=3, nel=16, NumFlux=2, ES=1, steps=100, CFL=0.4) -> Problem:
+    p = Params(N=N, CFL=CFL, T=1.0e9, g_const=9.81, NumFlux=NumFlux, ES=ES, rkOrder=4, rkSSP=0, MaxSteps=steps)
+    m = mesh_cartesian(N, 0.0, 2.0, 0.0, 2.0, nel, nel, True, True)
+    x, y = m.x, m.y
+    b = 0.1 * np.sin(np.pi * x) * np.cos(np.pi * y)
+    h = 1.0 - b + 0.05 * np.exp(-50.0 * ((x - 1.0) ** 2 + (y - 1.0) ** 2))
+    n2 = (N + 1) ** 2
+    return make_problem(p, m, b, _state(h, K=m.K, n2=n2), {"name": "periodic_bump", "nel": nel})
+
+
+def gaussian_bumps(x, y, seed, count=8):
+    rng = np.random.default_rng(seed)
+    b = np.zeros_like(x)
+    for _ in range(count):
+        amp = rng.uniform(0.05, 0.3)
+        w = rng.uniform(0.03, 0.1)
+        cx, cy = rng.uniform(0.0, 1.0, size=2)
+        b += amp * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (w * w))
+    return b
+
+
+def curved_lake(N=4, nel=512, seed=0, ripple=0.01, steps=1000, NumFlux=0, CFL=0.4, rotate_seed=0,
+                curve_order=None) -> Problem:
+    p = Params(N=N, CFL=CFL, T=1.0e9, g_const=9.81, NumFlux=NumFlux, ES=1, rkOrder=4, rkSSP=0, MaxSteps=steps)
+    m = mesh_mapped(N, 0.0, 1.0, 0.0, 1.0, nel, nel, amp=0.03, curve_order=curve_order, rotate_seed=rotate_seed)
+    x, y = m.x, m.y
+    b = gaussian_bumps(x, y, seed)
+    h = 1.0 - b
+    if ripple:
+        rng = np.random.default_rng(seed + 1000)
+        cx, cy = rng.uniform(0.25, 0.75, size=2)
+        w = rng.uniform(0.03, 0.08)
+        h = h + ripple * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (w * w))
+    n2 = (N + 1) ** 2
+    return make_problem(p, m, b, _state(h, K=m.K, n2=n2),
+                        {"name": "curved_lake", "nel": nel, "seed": seed, "ripple": ripple})
+
+
+def dam_break(N=4, nel=256, seed=0, steps=2000, NumFlux=0, CFL=0.4, AV=1, eps0=None, sigma_min=None,
+              sigma_max=None, PP=0, rotate_seed=0) -> Problem:
+    rng = np.random.default_rng(seed)
+    r0 = rng.uniform(0.2, 0.35)
+    cx, cy = rng.uniform(0.5 - 0.1, 0.5 + 0.1, size=2)
+    # eps0 is scaled like the reference's dam-break runs: O(h * lambda_max)
+    p = Params(N=N, CFL=CFL, DFL=0.1, T=1.0e9, g_const=9.81, NumFlux=NumFlux, ES=1, rkOrder=4, rkSSP=0,
+               ArtificialViscosity=AV, PositivityPreserving=PP, MaxSteps=steps,
+               epsilon_0=0.01 if eps0 is None else eps0,
+               sigma_min=-6.0 if sigma_min is None else sigma_min,
+               sigma_max=-2.0 if sigma_max is None else sigma_max)
+    m = mesh_mapped(N, 0.0, 1.0, 0.0, 1.0, nel, nel, amp=0.03, rotate_seed=rotate_seed)
+    x, y = m.x, m.y
+    b = np.zeros_like(x)
+    h = np.where((x - cx) ** 2 + (y - cy) ** 2 < r0 * r0, 2.0, 1.0)
+    n2 = (N + 1) ** 2
+    return make_problem(p, m, b, _state(h, K=m.K, n2=n2),
+                        {"name": "dam_break", "nel": nel, "seed": seed, "radius": r0, "centre": (cx, cy)})

@@ -1,0 +1,188 @@
+/*
+ * esdg_b200.h -- C ABI of the B200 ES-DGSEM shallow-water engine.
+ *
+ * The device entry points replace the OCCA-backed class `deviceclass` of
+ * ESDGSEM_MPIOCCA (include/deviceclass.h:28-138, src/deviceclass.cpp) one
+ * for one: same call order, same arguments (MPI/partition/basis objects are
+ * passed as the plain numbers the time loop reads from them), host arrays
+ * borrowed and copied, device buffers owned by the handle.  Every function
+ * returns 0 on success or a negative ESDG_E* code; esdg_last_error() gives
+ * the message.  Only plain C types cross this boundary.
+ *
+ * The set-up entry points (esdg_mesh_*, esdg_basis, ...) build the host
+ * arrays that the reference's main.cpp and src/{basis,Mesh,SW2D,
+ * MeshPartitioning,RungeKutta}.cpp build before calling deviceclass.
+ */
+#ifndef ESDG_B200_H
+#define ESDG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESDG_OK 0
+#define ESDG_E_ARG (-1)          /* bad argument or call order            */
+#define ESDG_E_UNSUPPORTED (-2)  /* option outside the rebuilt hot path   */
+#define ESDG_E_CUDA (-3)         /* CUDA runtime error                     */
+#define ESDG_E_NONFINITE (-4)    /* solution became NaN/inf (step stopped) */
+#define ESDG_E_IO (-5)           /* mesh / input file error                */
+#define ESDG_E_NOMEM (-6)        /* device allocation failed               */
+
+typedef struct esdg_deviceclass esdg_deviceclass;
+
+/* deviceclass::deviceclass(rank, argc, argv) -- include/deviceclass.h:31,
+ * src/deviceclass.cpp:20-103 (device selection).  device_id < 0 picks the
+ * current CUDA device. */
+int esdg_deviceclass_create(int rank, int device_id, esdg_deviceclass** out);
+
+/* deviceclass::initDeviceVariables -- include/deviceclass.h:32-57,
+ * src/deviceclass.cpp:108-345 (constants + device allocations). */
+int esdg_init_device_variables(esdg_deviceclass* d, int N, int Nelem, int Nfaces, int rank, int rkSSP, int NEpad,
+                               int NEsurfpad, int Nedgepad, int NAvgPad, int ES, int Testcase, double epsilon_0,
+                               double sigma_max, double sigma_min, double PosPresTOL, double geomface,
+                               double g_const, int PositivityPreserving, int ArtificialViscosity, int DiscBottom,
+                               double h_0, int PartialDry, int FrictionTerms, int CalcArrivalTimes,
+                               int CreateTimeSeries, int CalcMaximumElevation);
+
+/* deviceclass::copyDeviceVariables -- include/deviceclass.h:78-107,
+ * src/deviceclass.cpp:576-626.  Array sizes: K=Nelem elements, F faces,
+ * n=N+1: nodal [K*n*n], q/gRK/Qt [K*3*n*n], face [F*n], matrices [n*n],
+ * GLw [n], ElementSizes [K], element tables [K*4], EdgeData [F*8],
+ * EdgeReversed [F]. */
+int esdg_copy_device_variables(esdg_deviceclass* d, int PositivityPreserving, int Nelem, const double* GLw,
+                               const double* normalsX, const double* normalsY, const double* Scal,
+                               const double* y_xi, const double* y_eta, const double* x_xi, const double* x_eta,
+                               const double* b, const double* Bx, const double* By, const double* Dmat,
+                               const double* Dstrong, const double* Dhat, const double* J, const double* x_phy,
+                               const double* y_phy, const double* q, const double* ElementSizes, const double* gRK,
+                               const double* Qt, const double* VdmInv, const int* ElemEdgeMasterSlave,
+                               const int* ElemEdgeOrientation, const int* ElemToEdge, const int* EdgeData,
+                               const int* EdgeReversed);
+
+/* deviceclass::buildDeviceKernels -- include/deviceclass.h:60-68,
+ * src/deviceclass.cpp:349-544 (kernel selection; here: choice among the
+ * compiled sm_100a instantiations). */
+int esdg_build_device_kernels(esdg_deviceclass* d, int KernelVersion, int KernelVersionSTD, int Testcase,
+                              int FluxDifferencing, int NumFlux, int rkSSP, int ArtificialViscosity,
+                              int PositivityPreserving, int DiscBottom);
+
+/* deviceclass::DGtimeloop -- include/deviceclass.h:113-133,
+ * src/deviceclass.cpp:630-1335.  The RungeKutta object is passed as its
+ * tables (rkStages, CoeffsA/B/C); globalMinEleSize as computed by
+ * basis::calcElementSizes.  max_steps > 0 additionally caps the number of
+ * steps (the reference loop is time-driven only).  Plot/time-series
+ * arguments are accepted and ignored (no Tecplot output).  On return
+ * *t_out / *steps_out hold the reached time and the step count. */
+int esdg_dg_timeloop(esdg_deviceclass* d, int Nelem, int Nfaces, int rkStages, const double* rkA, const double* rkB,
+                     const double* rkC, double globalMinEleSize, double CFL, double DFL, double T, int Testcase,
+                     int ArtificialViscosity, int rkSSP, int NumPlots, int NumTimeChecks, double g_const,
+                     int PlotVar, int EntropyPlot, int PositivityPreserving, int DiscBottom, int max_steps,
+                     double* t_out, int* steps_out);
+
+/* occa_device.o_q.copyTo(q) -- main.cpp:1051. */
+int esdg_copy_q_to_host(esdg_deviceclass* d, double* q);
+/* o_q.copyFrom(q) for restarting from a host state (src/deviceclass.cpp:593). */
+int esdg_copy_q_from_host(esdg_deviceclass* d, const double* q);
+
+/* device.bytesAllocated() -- main.cpp:986. */
+long long esdg_bytes_allocated(const esdg_deviceclass* d);
+
+/* deviceclass::freeOccaVars -- include/deviceclass.h:108-110,
+ * src/deviceclass.cpp:1338-1420 (here: frees every device buffer). */
+int esdg_free_occa_vars(esdg_deviceclass* d, int rkSSP, int PositivityPreserving, int ArtificialViscosity);
+
+/* ~deviceclass. */
+int esdg_deviceclass_destroy(esdg_deviceclass* d);
+
+/* Message of the last failing call on this handle (or of the last failed
+ * create when d is NULL). */
+const char* esdg_last_error(const esdg_deviceclass* d);
+
+/* One right-hand-side evaluation Qt = L(q) of the current state, as the
+ * stage body of src/deviceclass.cpp:957-1094 computes it before the RK
+ * update (AV terms included when enabled).  Qt_host [K*3*n*n]; visc_host
+ * [K] (optional, AV only) receives the element viscosity used. */
+int esdg_compute_rhs(esdg_deviceclass* d, double* Qt_host, double* visc_host);
+
+/* Launch on the given cudaStream_t (NULL restores the handle's own stream).
+ * Lets a caller order the engine's kernels with its own work and time them
+ * with its own events. */
+int esdg_set_stream(esdg_deviceclass* d, void* cuda_stream);
+
+/* Advance the resident state by up to nsteps steps (same step as
+ * esdg_dg_timeloop) without any host copy of q; the device-side time and
+ * step count continue from the previous call.  T is the end time. */
+int esdg_advance(esdg_deviceclass* d, int nsteps, double T, double* t_out, int* steps_out);
+
+/* Advance nsteps real steps launching kernel by kernel (no graph) with CUDA
+ * events recorded on the launching stream around the face-flux and the
+ * element launches; returns their average durations in ms per stage. */
+int esdg_profile_steps(esdg_deviceclass* d, int nsteps, double* face_ms, double* elem_ms);
+
+/* Element viscosity of the last step (AV only) [K]. */
+int esdg_copy_visc_to_host(esdg_deviceclass* d, double* visc);
+
+/* Number of kernel launches issued by the engine since creation (graph
+ * replays count the kernels inside the graph). */
+long long esdg_kernel_launches(const esdg_deviceclass* d);
+
+/* ------------------------------------------------------------------------
+ * Host set-up (no GPU needed).
+ * ---------------------------------------------------------------------- */
+
+typedef struct esdg_mesh esdg_mesh;
+
+/* basis::basis (src/basis.cpp:28-188): LGL nodes/weights [n], Gauss
+ * nodes/weights [n], D (flux-differencing form when FluxDifferencing),
+ * D0 (plain collocation derivative), Dstrong, Dhat, VdmInv [n*n]. */
+int esdg_basis(int N, int FluxDifferencing, double* xGL, double* wGL, double* xG, double* wG, double* D, double* D0,
+               double* Dstrong, double* Dhat, double* VdmInv);
+
+/* Mesh::GenerateMesh (src/Mesh.cpp:316-696) for a Cartesian grid.
+ * periodic_rows / periodic_cols are the reference's PeriodicBD_X /
+ * PeriodicBD_Y (wrap of the horizontal / vertical faces). */
+int esdg_mesh_cartesian(int N, double xL, double xR, double yL, double yR, int NX, int NY, int periodic_rows,
+                        int periodic_cols, esdg_mesh** out);
+
+/* Structured curved grid x -> x + amp*Lx*sin(2pi(x-xL)/Lx)sin(2pi(y-yL)/Ly)
+ * (y likewise) with every side given as an order-m boundary curve, i.e. the
+ * ISM-V2 mesh that esdg_mesh_write_ism2 writes; rotate_seed != 0 rotates
+ * element corner numbering pseudo-randomly (faces of all orientations). */
+int esdg_mesh_mapped(int N, double xL, double xR, double yL, double yR, int NX, int NY, double amp, int m,
+                     unsigned rotate_seed, esdg_mesh** out);
+
+/* Mesh::ReadMesh (src/Mesh.cpp:698-1503): ISM-V2 reader. */
+int esdg_mesh_read_ism2(int N, const char* path, int read_bottom, int convert_km, esdg_mesh** out);
+int esdg_mesh_write_ism2(const esdg_mesh* m, const char* path);
+
+/* Element and face counts. */
+int esdg_mesh_sizes(const esdg_mesh* m, int* K, int* F);
+
+/* Arrays as main.cpp:650-716 hands them to copyDeviceVariables (J is 1/J).
+ * Any pointer may be NULL. */
+int esdg_mesh_pack(const esdg_mesh* m, double* x, double* y, double* x_xi, double* x_eta, double* y_xi,
+                   double* y_eta, double* Jinv, double* nx, double* ny, double* scal, double* b, int* EdgeData,
+                   int* EdgeReversed, int* ElemToEdge, int* ElemEdgeMasterSlave, int* ElemEdgeOrientation);
+void esdg_mesh_free(esdg_mesh* m);
+
+/* SW2D::CalcBDerivatives (src/SW2D.cpp:1048-1105), Jinv = 1/J. */
+int esdg_bottom_derivatives(int K, int N, const double* D0, const double* b, const double* y_eta, const double* y_xi,
+                            const double* x_eta, const double* x_xi, const double* Jinv, double* Bx, double* By);
+
+/* basis::calcElementSizes (src/basis.cpp:939-966); returns sqrt(min area)
+ * in *minEleSize. */
+int esdg_element_sizes(int K, int N, const double* wGL, const double* Jinv, double* EleSizes, double* minEleSize);
+
+/* RungeKutta::RungeKutta (src/RungeKutta.cpp:18-90); A/B/C hold >= 5. */
+int esdg_rk_coefficients(int order, int ssp, double* A, double* B, double* C, int* stages);
+
+/* basis::L2Norm / LinfNorm / calcTotalMass / calcTotalEntropy
+ * (src/basis.cpp:874-1111); qref may be NULL (then L2/Linf are skipped). */
+int esdg_diagnostics(int K, int N, const double* wGL, const double* Jinv, const double* q, const double* qref,
+                     const double* b, double g, double* L2, double* Linf, double* mass, double* entropy);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ESDG_B200_H */

@@ -1,0 +1,161 @@
+"""CUDA engine vs CPU oracle on the same seeded inputs (GPU).
+
+Tolerances (FP64 throughout; the engine contracts a*b+c into FMA, the oracle
+does not, so results differ at round-off and grow slowly with the steps):
+  * one right-hand side:        max|dQt| <= 1e-13 * S per variable, S the
+                                largest term that enters it (max|Qt|, g*h*|grad b|,
+                                and 1), since the flux and source terms cancel
+  * 100 LS-RK4 steps:           relative L2 per conserved variable <= 1e-12
+  * lake at rest:               max|h+b-1| <= 1e-13; max|hu|, max|hv| within
+                                10x of the oracle's own round-off drift
+"""
+import numpy as np
+import pytest
+
+from esdgsem_mpiocca_b200 import problems
+from esdgsem_mpiocca_b200.deviceclass import EsdgError, Solver, E_UNSUPPORTED
+from oracle.oracle import OracleProblem
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2_per_var(a, b, K, n2):
+    a = a.reshape(K, 3, n2)
+    b = b.reshape(K, 3, n2)
+    out = []
+    for v in range(3):
+        den = np.linalg.norm(b[:, v])
+        out.append(np.linalg.norm(a[:, v] - b[:, v]) / (den if den > 0 else 1.0))
+    return out
+
+
+def term_scale(pr):
+    """Size of the largest single term of the flux-differencing sum,
+    Jinv * |D| * (|f| + |g|) * |metric|, before the terms cancel."""
+    K, n2 = pr.K, pr.ngl ** 2
+    q = pr.q0.reshape(K, 3, n2)
+    h, hu, hv = q[:, 0], q[:, 1], q[:, 2]
+    hmin = max(h.min(), 1e-3)
+    flux = 0.5 * pr.params.g_const * (h ** 2).max() + ((hu ** 2).max() + (hv ** 2).max()) / hmin
+    met = max(np.abs(a).max() for a in (pr.mesh.x_xi, pr.mesh.x_eta, pr.mesh.y_xi, pr.mesh.y_eta))
+    return pr.mesh.Jinv.max() * np.abs(pr.basis.D).max() * flux * met
+
+
+def assert_rhs_close(Qg, Qo, pr, rtol=1e-13):
+    K, n2 = pr.K, pr.ngl ** 2
+    a = Qg.reshape(K, 3, n2)
+    b = Qo.reshape(K, 3, n2)
+    S = term_scale(pr)
+    for v in range(3):
+        err = np.abs(a[:, v] - b[:, v]).max() / max(S, np.abs(b[:, v]).max())
+        assert err <= rtol, (v, err)
+
+
+@pytest.mark.parametrize("numflux", [0, 2, 3])
+def test_rhs_periodic(numflux):
+    pr = problems.periodic_bump(NumFlux=numflux)
+    s = Solver(pr)
+    try:
+        Qg = s.rhs()
+    finally:
+        s.close()
+    Qo = OracleProblem(pr).rhs(pr.q0)
+    assert_rhs_close(Qg, Qo, pr)
+
+
+@pytest.mark.parametrize("numflux,N", [(0, 4), (3, 3), (2, 4)])
+def test_rhs_curved_rotated_walls(numflux, N):
+    # corner rotations give faces of every orientation pairing
+    pr = problems.curved_lake(N=N, nel=12, seed=3, ripple=0.02, NumFlux=numflux, rotate_seed=7)
+    assert (pr.mesh.EdgeReversed == 0).any()
+    s = Solver(pr)
+    try:
+        Qg = s.rhs()
+    finally:
+        s.close()
+    Qo = OracleProblem(pr).rhs(pr.q0)
+    assert_rhs_close(Qg, Qo, pr)
+
+
+@pytest.mark.parametrize("numflux", [2, 0, 3])
+def test_timeloop_periodic_100_steps(numflux):
+    pr = problems.periodic_bump(NumFlux=numflux, steps=100)
+    s = Solver(pr)
+    try:
+        t, steps = s.run()
+        qg = s.q()
+    finally:
+        s.close()
+    ref = OracleProblem(pr).run()
+    assert steps == ref["steps"] == 100
+    assert abs(t - ref["t"]) <= 1e-13 * ref["t"]
+    errs = rel_l2_per_var(qg, ref["q"], pr.K, pr.ngl ** 2)
+    assert max(errs) <= 1e-12, errs
+
+
+def test_timeloop_curved_walls_100_steps():
+    pr = problems.curved_lake(N=4, nel=16, seed=1, ripple=0.05, steps=100, rotate_seed=11)
+    s = Solver(pr)
+    try:
+        t, steps = s.run()
+        qg = s.q()
+    finally:
+        s.close()
+    ref = OracleProblem(pr).run()
+    assert steps == ref["steps"] == 100
+    errs = rel_l2_per_var(qg, ref["q"], pr.K, pr.ngl ** 2)
+    assert max(errs) <= 1e-12, errs
+
+
+def test_time_driven_loop_stops_at_T():
+    pr = problems.periodic_bump(NumFlux=0, steps=0)
+    T = 0.05
+    s = Solver(pr)
+    try:
+        t, steps = s.run(T=T, max_steps=0)
+        qg = s.q()
+    finally:
+        s.close()
+    ref = OracleProblem(pr).run(T=T, max_steps=0)
+    assert steps == ref["steps"]
+    assert t == pytest.approx(T, abs=1e-15)
+    assert max(rel_l2_per_var(qg, ref["q"], pr.K, pr.ngl ** 2)) <= 1e-12
+
+
+def test_lake_at_rest_curved():
+    pr = problems.curved_lake(N=4, nel=16, seed=5, ripple=0.0, steps=50, rotate_seed=3)
+    s = Solver(pr)
+    try:
+        s.run()
+        q = s.q().reshape(pr.K, 3, -1)
+    finally:
+        s.close()
+    b = pr.b.reshape(pr.K, -1)
+    ref = OracleProblem(pr).run()["q"].reshape(pr.K, 3, -1)
+    assert np.abs(q[:, 0] + b - 1.0).max() <= 1e-13
+    for v in (1, 2):
+        drift = np.abs(ref[:, v]).max()
+        assert np.abs(q[:, v]).max() <= 10 * drift + 1e-15, (v, np.abs(q[:, v]).max(), drift)
+
+
+def test_ssp_rk3_matches_oracle():
+    pr = problems.periodic_bump(NumFlux=0, steps=40)
+    pr.params.rkOrder, pr.params.rkSSP = 3, 1
+    from esdgsem_mpiocca_b200.host import rk_coefficients
+    pr.rkA, pr.rkB, pr.rkC = rk_coefficients(3, 1)
+    s = Solver(pr)
+    try:
+        s.run()
+        qg = s.q()
+    finally:
+        s.close()
+    ref = OracleProblem(pr).run()
+    assert max(rel_l2_per_var(qg, ref["q"], pr.K, pr.ngl ** 2)) <= 1e-12
+
+
+def test_unsupported_options_fail_loudly():
+    pr = problems.periodic_bump()
+    pr.params.NumFlux = 1  # Lax-Friedrichs: not entropy stable, not rebuilt
+    with pytest.raises(EsdgError) as ei:
+        Solver(pr)
+    assert ei.value.code == E_UNSUPPORTED
