@@ -205,7 +205,7 @@ void build_basis(int N, int flux_differencing, Basis* B) {
             Vtmp[j * n + i] = L * std::sqrt(j + 0.5) * B->wG[i];
         }
     for (int i = 0; i < n; ++i) {
-        lagrange_basis_at(B->xG[i], N, B->xGL.data(), B->wbary.data(), P.data());
+        lagrange_basis_at(B->xG[i], n, B->xGL.data(), B->wbary.data(), P.data());
         for (int j = 0; j < n; ++j) Itmp[i * n + j] = P[j];
     }
     for (int i = 0; i < n; ++i)

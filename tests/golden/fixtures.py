@@ -1,0 +1,40 @@
+"""Loads the golden fixtures written by make_golden.py into host.Problem
+objects (the arrays exactly as the reference handed them to its device
+layer) plus the reference's final state."""
+from __future__ import annotations
+
+import glob
+import json
+import os
+
+import numpy as np
+
+from esdgsem_mpiocca_b200 import host
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.npz")))
+
+
+def load(name):
+    z = np.load(os.path.join(HERE, f"{name}.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    p = host.Params(**meta["params"])
+    N = p.N
+    n2 = (N + 1) ** 2
+    K = z["Jinv"].size // n2
+    F = z["EdgeReversed"].size
+    mesh = host.MeshArrays(N, K, F, z["x"], z["y"], z["x_xi"], z["x_eta"], z["y_xi"], z["y_eta"], z["Jinv"],
+                           z["nx"], z["ny"], z["scal"], z["b"], z["EdgeData"].astype(np.int32),
+                           z["EdgeReversed"].astype(np.int32), z["ElemToEdge"].astype(np.int32),
+                           z["MasterSlave"].astype(np.int32), z["Orientation"].astype(np.int32))
+    basis = host.Basis.build(N, p.FluxDifferencing)
+    # the matrices the reference used (identical to basis' -- checked by tests)
+    basis.D, basis.Dstrong, basis.Dhat, basis.VdmInv = z["D"], z["Dstrong"], z["Dhat"], z["VdmInv"]
+    EleSizes = z["EleSizes"]
+    minEle = float(np.sqrt(EleSizes.min()))
+    prob = host.Problem(p, basis, mesh, z["b"], z["Bx"], z["By"], z["q"], EleSizes, minEle, z["rkA"], z["rkB"],
+                        z["rkC"], meta)
+    return prob, z["q_final"], z

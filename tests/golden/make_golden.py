@@ -1,0 +1,167 @@
+"""Generates the golden fixtures in tests/golden/*.npz from runs of the
+reference program itself (oracle/_ref/esdg_ref: the reference's main.cpp and
+src/*.cpp compiled unmodified against the OCCA-v0 shim, kernels from its own
+okl/ files).  Run in a container that has the reference tree:
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py CASE ...   # selected cases
+
+Each fixture holds every array the reference handed to copyDeviceVariables
+(its own set-up, or the injected initial state / bathymetry), the time-loop
+parameters, and q after its DGtimeloop (o_q.copyTo at main.cpp:1051).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from esdgsem_mpiocca_b200 import host, problems  # noqa: E402
+from oracle import run_ref  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def gaussian_state(x, y, seed, depth=1.0, ripple=0.02, nb=3):
+    rng = np.random.default_rng(seed)
+    lx, ly = x.max() - x.min(), y.max() - y.min()
+    b = np.zeros_like(x)
+    for _ in range(nb):
+        a = rng.uniform(0.05, 0.2)
+        w = rng.uniform(0.1, 0.25) * min(lx, ly)
+        cx = rng.uniform(x.min(), x.max())
+        cy = rng.uniform(y.min(), y.max())
+        b += a * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / w ** 2)
+    cx, cy = x.min() + 0.4 * lx, y.min() + 0.55 * ly
+    h = depth - b + ripple * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (0.15 * min(lx, ly)) ** 2)
+    return b, h
+
+
+def pack_q(h, hu=None, hv=None, n2=None):
+    K = h.size // n2
+    q = np.zeros((K, 3, n2))
+    q[:, 0] = h.reshape(K, n2)
+    if hu is not None:
+        q[:, 1] = hu.reshape(K, n2)
+    if hv is not None:
+        q[:, 2] = hv.reshape(K, n2)
+    return q.reshape(-1)
+
+
+def bottom_derivs(ref_setup, N, b):
+    """Bx, By of b on the reference's own geometry (its CalcBDerivatives is
+    bypassed by injection, so they are recomputed here on its arrays)."""
+    K = ref_setup["Jinv"].size // (N + 1) ** 2
+    mesh = host.MeshArrays(N, K, ref_setup["EdgeReversed"].size, ref_setup["x"], ref_setup["y"], ref_setup["x_xi"],
+                           ref_setup["x_eta"], ref_setup["y_xi"], ref_setup["y_eta"], ref_setup["Jinv"],
+                           ref_setup["nx"], ref_setup["ny"], ref_setup["scal"], b, ref_setup["EdgeData"],
+                           ref_setup["EdgeReversed"], ref_setup["ElemToEdge"], ref_setup["MasterSlave"],
+                           ref_setup["Orientation"])
+    return host.bottom_derivatives(mesh, host.Basis.build(N), b)
+
+
+def save(name, params, out, meta):
+    arrays = {k: v for k, v in out.items() if isinstance(v, np.ndarray)}
+    rk = host.rk_coefficients(params.rkOrder, params.rkSSP)
+    arrays["rkA"], arrays["rkB"], arrays["rkC"] = rk
+    p = {k: getattr(params, k) for k in vars(params)}
+    meta = dict(meta)
+    meta["params"] = p
+    meta["reference_stdout_tail"] = out["stdout"][-400:]
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **arrays)
+    print(f"{name}: K={out['Jinv'].size // (params.N + 1) ** 2} wall={out['wall']:.2f}s")
+
+
+def case_periodic(numflux, name):
+    pr = problems.periodic_bump(NumFlux=numflux, steps=0)
+    pr.params.T = 0.1
+    out = run_ref.run(name, pr.params, cartesian=(0.0, 2.0, 0.0, 2.0, 16, 16, 1, 1),
+                      inject={"q": pr.q0, "b": pr.b, "Bx": pr.Bx, "By": pr.By})
+    save(name, pr.params, out, {"mesh": "Cartesian periodic 16x16 on [0,2]^2", "state": "periodic_bump"})
+
+
+def case_mapped_rotated(name="mapped_rot_N4", N=4):
+    """Curved 8x8 mesh with rotated element corners, written as ISM-V2 by the
+    engine's writer and read by the reference's Mesh::ReadMesh."""
+    params = host.Params(N=N, CFL=0.4, T=0.02, NumFlux=0, rkOrder=4, rkSSP=0)
+    rd = os.path.join(ROOT, "oracle", "_ref", "meshes")
+    os.makedirs(rd, exist_ok=True)
+    path = os.path.join(rd, "mapped_rot.mesh")
+    m = host.mesh_mapped(N, 0.0, 1.0, 0.0, 1.0, 8, 8, amp=0.03, curve_order=5, rotate_seed=7, write_path=path)
+    b, h = gaussian_state(m.x, m.y, seed=11)
+    setup = run_ref.run(name + "_setup", params, mesh_file=path)
+    Bx, By = bottom_derivs(setup, N, b)
+    out = run_ref.run(name, params, mesh_file=path, inject={"q": pack_q(h, n2=(N + 1) ** 2), "b": b, "Bx": Bx,
+                                                            "By": By})
+    save(name, params, out, {"mesh": "engine-written ISM-V2: curved 8x8, rotated corners, order 5", "walls": True})
+
+
+def case_circle(name, N=3, AV=0, T=0.01, state="lake"):
+    params = host.Params(N=N, CFL=0.4, DFL=0.1, T=T, NumFlux=0, rkOrder=4, rkSSP=0, ArtificialViscosity=AV,
+                         epsilon_0=0.02, sigma_min=-6.0, sigma_max=-2.0)
+    mf = "meshFiles/CircleInCircle.mesh"
+    setup = run_ref.run(name + "_setup", params, mesh_file=mf)
+    x, y = setup["x"], setup["y"]
+    if state == "lake":
+        b, h = gaussian_state(x, y, seed=5)
+    else:  # circular dam on a flat bottom
+        b = np.zeros_like(x)
+        cx, cy = np.median(x), np.median(y)
+        r = 0.3 * (x.max() - x.min())
+        h = np.where((x - cx) ** 2 + (y - cy) ** 2 < r * r, 2.0, 1.0)
+    Bx, By = bottom_derivs(setup, N, b)
+    out = run_ref.run(name, params, mesh_file=mf, inject={"q": pack_q(h, n2=(N + 1) ** 2), "b": b, "Bx": Bx,
+                                                          "By": By})
+    save(name, params, out, {"mesh": "reference meshFiles/CircleInCircle.mesh (curved order 6, 83 reversed faces)",
+                             "state": state})
+
+
+def case_positivity(name="periodic_pp_N3"):
+    pr = problems.periodic_bump(NumFlux=0, steps=0)
+    pr.params.PositivityPreserving = 1
+    pr.params.PosPresTOL = 1e-3
+    pr.params.T = 0.01
+    q = pr.q0.reshape(pr.K, 3, -1).copy()
+    xi = np.tile(np.linspace(-1.0, 1.0, pr.ngl), pr.ngl)
+    for e in (3, 77, 150):
+        q[e, 0] = 0.01
+        q[e, 1] = 0.01 * 5.0 * xi
+    out = run_ref.run(name, pr.params, cartesian=(0.0, 2.0, 0.0, 2.0, 16, 16, 1, 1),
+                      inject={"q": q.reshape(-1), "b": pr.b, "Bx": pr.Bx, "By": pr.By})
+    save(name, pr.params, out, {"mesh": "Cartesian periodic 16x16", "state": "draining shallow elements"})
+
+
+def case_ssp_walls(name="walls_ssp3_N2"):
+    N = 2
+    params = host.Params(N=N, CFL=0.3, T=0.05, NumFlux=3, rkOrder=3, rkSSP=1)
+    m = host.mesh_cartesian(N, -1.0, 1.0, 0.0, 1.0, 10, 8)
+    b, h = gaussian_state(m.x, m.y, seed=9)
+    basis = host.Basis.build(N)
+    Bx, By = host.bottom_derivatives(m, basis, b)
+    out = run_ref.run(name, params, cartesian=(-1.0, 1.0, 0.0, 1.0, 10, 8, 0, 0),
+                      inject={"q": pack_q(h, n2=(N + 1) ** 2), "b": b, "Bx": Bx, "By": By})
+    save(name, params, out, {"mesh": "Cartesian walls 10x8 on [-1,1]x[0,1]", "rk": "SSP-RK3"})
+
+
+CASES = {
+    "periodic_nf0_N3": lambda: case_periodic(0, "periodic_nf0_N3"),
+    "periodic_nf3_N3": lambda: case_periodic(3, "periodic_nf3_N3"),
+    "mapped_rot_N4": lambda: case_mapped_rotated(),
+    "circle_lake_N3": lambda: case_circle("circle_lake_N3", N=3, T=0.01, state="lake"),
+    "circle_dam_av_N3": lambda: case_circle("circle_dam_av_N3", N=3, AV=1, T=0.005, state="dam"),
+    "periodic_pp_N3": lambda: case_positivity(),
+    "walls_ssp3_N2": lambda: case_ssp_walls(),
+}
+
+if __name__ == "__main__":
+    if not run_ref.available():
+        sys.exit("the reference tree is not available here")
+    run_ref.build()
+    for c in (sys.argv[1:] or list(CASES)):
+        CASES[c]()

@@ -1,0 +1,100 @@
+"""Pins the oracle and the host set-up to the reference itself (CPU).
+
+The fixtures in tests/golden/ come from runs of the reference program
+(tests/golden/make_golden.py).  Required here:
+  * the oracle started from the reference's own copyDeviceVariables arrays
+    ends in exactly the reference's final state (bit for bit: both are plain
+    double arithmetic in the same order, no FMA contraction);
+  * the engine's host set-up (basis, Cartesian generator, ISM-V2 reader of
+    its own curved meshes, element sizes, packed tables) reproduces the
+    reference's set-up arrays bit for bit.
+"""
+import numpy as np
+import pytest
+
+from esdgsem_mpiocca_b200 import host
+from oracle.oracle import OracleProblem
+from tests.golden import fixtures
+
+CASES = fixtures.names()
+
+
+def test_fixtures_present():
+    assert len(CASES) >= 7
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_reproduces_reference_bitwise(name):
+    prob, q_ref, _ = fixtures.load(name)
+    out = OracleProblem(prob).run(T=prob.params.T, max_steps=0)
+    assert out["steps"] > 0
+    assert np.isfinite(q_ref).all()
+    np.testing.assert_array_equal(out["q"], q_ref)
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_basis_matches_reference(N):
+    name = {2: "walls_ssp3_N2", 3: "periodic_nf0_N3", 4: "mapped_rot_N4"}[N]
+    _, _, z = fixtures.load(name)
+    b = host.Basis.build(N)
+    for k, mine in (("D", b.D), ("Dstrong", b.Dstrong), ("Dhat", b.Dhat), ("VdmInv", b.VdmInv)):
+        np.testing.assert_array_equal(mine, z[k], err_msg=k)
+
+
+def _compare_setup(mesh, basis, z, skip=()):
+    es, _ = host.element_sizes(mesh, basis)
+    pairs = [("nx", mesh.nx), ("ny", mesh.ny), ("scal", mesh.scal), ("x_xi", mesh.x_xi), ("x_eta", mesh.x_eta),
+             ("y_xi", mesh.y_xi), ("y_eta", mesh.y_eta), ("Jinv", mesh.Jinv), ("x", mesh.x), ("y", mesh.y),
+             ("EleSizes", es), ("EdgeData", mesh.EdgeData), ("EdgeReversed", mesh.EdgeReversed),
+             ("ElemToEdge", mesh.ElemToEdge), ("MasterSlave", mesh.MasterSlave), ("Orientation", mesh.Orientation)]
+    for k, mine in pairs:
+        if k in skip:
+            continue
+        np.testing.assert_array_equal(mine, z[k].astype(mine.dtype), err_msg=k)
+
+
+@pytest.mark.parametrize("name,args", [
+    ("periodic_nf0_N3", (3, 0.0, 2.0, 0.0, 2.0, 16, 16, True, True)),
+    ("walls_ssp3_N2", (2, -1.0, 1.0, 0.0, 1.0, 10, 8, False, False)),
+])
+def test_cartesian_setup_matches_reference(name, args):
+    _, _, z = fixtures.load(name)
+    mesh = host.mesh_cartesian(*args)
+    _compare_setup(mesh, host.Basis.build(args[0]), z)
+
+
+def test_curved_rotated_setup_matches_reference_reader():
+    # the reference read the ISM-V2 file that this generator writes
+    _, _, z = fixtures.load("mapped_rot_N4")
+    mesh = host.mesh_mapped(4, 0.0, 1.0, 0.0, 1.0, 8, 8, amp=0.03, curve_order=5, rotate_seed=7)
+    assert (mesh.EdgeReversed == 0).any()
+    _compare_setup(mesh, host.Basis.build(4), z)
+
+
+def test_ism2_roundtrip(tmp_path):
+    p = tmp_path / "m.mesh"
+    a = host.mesh_mapped(3, 0.0, 2.0, -1.0, 1.0, 5, 4, amp=0.05, curve_order=4, rotate_seed=3, write_path=p)
+    b = host.mesh_read(3, p)
+    for k in ("x", "y", "x_xi", "x_eta", "y_xi", "y_eta", "Jinv", "nx", "ny", "scal", "EdgeData", "ElemToEdge",
+              "MasterSlave", "Orientation", "EdgeReversed"):
+        np.testing.assert_array_equal(getattr(a, k), getattr(b, k), err_msg=k)
+
+
+def test_bottom_derivatives_match_reference_algorithm():
+    # Bx/By recomputed on the reference's geometry equal the injected ones
+    prob, _, z = fixtures.load("circle_lake_N3")
+    Bx, By = host.bottom_derivatives(prob.mesh, prob.basis, z["b"])
+    np.testing.assert_array_equal(Bx, z["Bx"])
+    np.testing.assert_array_equal(By, z["By"])
+
+
+@pytest.mark.skipif(not __import__("oracle.run_ref", fromlist=["available"]).available(),
+                    reason="reference tree not present")
+def test_reader_matches_reference_on_shipped_curved_mesh():
+    """Mesh::ReadMesh on the reference's own CircleInCircle.mesh (curved
+    boundaries of order 6, 83 reversed faces) vs the engine's reader."""
+    import os
+    from oracle import run_ref
+    _, _, z = fixtures.load("circle_lake_N3")
+    mesh = host.mesh_read(3, os.path.join(run_ref.REF, "meshFiles", "CircleInCircle.mesh"))
+    _compare_setup(mesh, host.Basis.build(3), z)
