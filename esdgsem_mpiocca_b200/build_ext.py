@@ -17,6 +17,9 @@ SOURCES = ["esdg_engine.cu", "esdg_ensemble.cu", "esdg_setup.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
+    # no a*b+c contraction: every FP64 operation rounds as in the reference's
+    # Serial/OpenMP build, so results match it bit for bit on the plain path
+    "-fmad=false",
     "-Xcompiler", "-fPIC,-O2",
     "-ccbin", "g++",
 ]

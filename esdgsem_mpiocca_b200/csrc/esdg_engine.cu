@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +26,7 @@
 
 #include "../../include/esdg_b200.h"
 #include "esdg_kernels.cuh"
+#include "esdg_tma.cuh"
 #include "esdg_setup.hpp"
 
 namespace esdg {
@@ -268,6 +270,17 @@ class Engine {
             return fail(ESDG_E_ARG, "buildDeviceKernels flags differ from initDeviceVariables");
         NumFlux = NumFlux_;
         FluxDiff = FluxDifferencing;
+        int r = 0;
+        switch (ngl) {
+            case 2: r = setup_tma<2>(); break;
+            case 3: r = setup_tma<3>(); break;
+            case 4: r = setup_tma<4>(); break;
+            case 5: r = setup_tma<5>(); break;
+            case 6: r = setup_tma<6>(); break;
+            case 7: r = setup_tma<7>(); break;
+            case 8: r = setup_tma<8>(); break;
+        }
+        if (r) return r;
         built = true;
         return 0;
     }
@@ -301,6 +314,40 @@ class Engine {
         return a;
     }
 
+    // Plain-path element kernel: the TMA-pipelined persistent kernel when the
+    // element count allows 16-byte bulk granularity, else the one-shot one.
+    int tma_grid = 0;  // persistent grid size (0: not set up / not usable)
+
+    template <int NGL>
+    int setup_tma() {
+        using T = TmaShape<NGL>;
+        tma_grid = 0;
+        if (((long long)K * T::N2) % 2 != 0) return 0;
+        cudaError_t e = cudaFuncSetAttribute(k_element_tma<NGL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)T::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_element_tma<NGL>, T::THREADS, T::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+        const int ntiles = (K + T::NE - 1) / T::NE;
+        tma_grid = std::max(1, std::min(ntiles, std::max(per_sm, 1) * sms));
+        return 0;
+    }
+
+    template <int NGL>
+    void launch_elem_plain(const ElemArgs& ea) {
+        if (tma_grid > 0) {
+            using T = TmaShape<NGL>;
+            k_element_tma<NGL><<<tma_grid, T::THREADS, T::SMEM, stream>>>(ea, (K + T::NE - 1) / T::NE);
+        } else {
+            using S = ElemShape<NGL>;
+            k_element<NGL><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, stream>>>(ea);
+        }
+        ++launches;
+    }
+
     template <int NGL>
     void launch_stage(int mode, double A, double Bc, double C, bool last, bool shock_stage) {
         using S = ElemShape<NGL>;
@@ -308,8 +355,7 @@ class Engine {
         const int lam_in_elem = (last && !PP) ? 1 : 0;
         launch_face<NGL>(AV != 0);
         if (!AV) {
-            k_element<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
-            ++launches;
+            launch_elem_plain<NGL>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
         } else {
             k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0, shock_stage ? 1 : 0));
             const long n = (long)F * NGL;
@@ -448,6 +494,7 @@ class Engine {
         if (st_host->status == ST_NONFINITE)
             return fail(ESDG_E_NONFINITE, "non-finite wave speed: the solution blew up (step " +
                                               std::to_string(st_host->steps) + ")");
+        if (st_host->status == ST_TIMEOUT) return fail(ESDG_E_CUDA, "a bulk copy did not complete (bounded wait)");
         return 0;
     }
 
@@ -501,8 +548,7 @@ class Engine {
             launch_face<NGL>(AV != 0);
             cudaEventRecord(pev[1], stream);
             if (!AV) {
-                k_element<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
-                ++launches;
+                launch_elem_plain<NGL>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
             } else {
                 k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0, s > 0));
                 const long n = (long)F * NGL;

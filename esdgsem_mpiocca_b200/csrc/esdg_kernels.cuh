@@ -247,20 +247,48 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
     const bool inb = e < a.K;
     const int ins = inb ? inst_of(a.elem_inst, e) : 0;
     const bool active = inb && !a.st[ins].done;
+    const int xi = nd % NGL, eta = nd / NGL;
     if (tid < N2) sD[tid] = a.D[tid];
     const long xid = (long)e * N2 + nd, qid = (long)e * 3 * N2 + nd;
-    double h = 0, hu = 0, hv = 0;
     const int s = el * N2 + nd;
+    // Every global read of this thread is issued here, before the barrier,
+    // so that their latencies overlap: state and metrics (staged for the
+    // partners), Jinv/Bx/By, gRK (or Qtmp) and the face fluxes of the
+    // node's sides.
+    double h = 0, hu = 0, hv = 0, J = 0, bx = 0, by = 0, o0 = 0, o1 = 0, o2 = 0, dt = 0;
+    double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    int ms[2] = {0, 0};
     if (active) {
         h = a.q[qid]; hu = a.q[qid + N2]; hv = a.q[qid + 2 * N2];
         sh[s] = h; shu[s] = hu; shv[s] = hv;
-        si[s] = (h > 0) ? 1.0 / h : 0.0;
         sYe[s] = a.Yeta[xid]; sYx[s] = a.Yxi[xid]; sXe[s] = a.Xeta[xid]; sXx[s] = a.Xxi[xid];
+        J = a.Jinv[xid]; bx = a.Bx[xid]; by = a.By[xid];
+        if (a.mode == 0) { o0 = a.gRK[qid]; o1 = a.gRK[qid + N2]; o2 = a.gRK[qid + 2 * N2]; }
+        else if (a.mode == 1) { o0 = a.Qtmp[qid]; o1 = a.Qtmp[qid + N2]; o2 = a.Qtmp[qid + 2 * N2]; }
+        if (a.mode != 2) dt = a.st[ins].dt;
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            int side = -1, j = 0;
+            if (pass == 0) {
+                if (eta == 0) { side = 0; j = xi; }
+                else if (eta == NGL - 1) { side = 2; j = xi; }
+            } else {
+                if (xi == NGL - 1) { side = 1; j = eta; }
+                else if (xi == 0) { side = 3; j = eta; }
+            }
+            if (side >= 0) {
+                const int4 sd = a.side[(long)e * 4 + side];
+                const int inc = sd.z ? j : NGL - 1 - j;
+                const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
+                ms[pass] = sd.y;
+                f[pass][0] = fp[0]; f[pass][1] = fp[NGL]; f[pass][2] = fp[2 * NGL];
+            }
+        }
+        si[s] = (h > 0) ? 1.0 / h : 0.0;
     }
     __syncthreads();
     double lam = 0.0;
     if (active) {
-        const int xi = nd % NGL, eta = nd / NGL;
         const int rb = el * N2 + eta * NGL;  // row base (same eta)
         const int cb = el * N2 + xi;         // column base (same xi)
         const double ih = si[s], ye = sYe[s], yx = sYx[s], xe = sXe[s], xx = sXx[s];
@@ -282,49 +310,36 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
             two_point_eta(fg, hg, h, hu, hv, ih, sh[p], shu[p], shv[p], si[p], yx, sYx[p], xx, sXx[p], g1, g2, g3);
             d1 += dl * g1; d2 += dl * g2; d3 += dl * g3;
         }
-        const double J = a.Jinv[xid];
         double r0 = -J * d1;
-        double r1 = -J * d2 - a.c.g * h * a.Bx[xid];
-        double r2 = -J * d3 - a.c.g * h * a.By[xid];
-        // lift: sides 0/2 first, then 1/3
+        double r1 = -J * d2 - a.c.g * h * bx;
+        double r2 = -J * d3 - a.c.g * h * by;
+        // lift: sides 0/2 first, then 1/3 (DBSurf1/2 are zero)
+        const double db = 0.0;
 #pragma unroll
         for (int pass = 0; pass < 2; ++pass) {
-            int side = -1, j = 0;
-            if (pass == 0) {
-                if (eta == 0) { side = 0; j = xi; }
-                else if (eta == NGL - 1) { side = 2; j = xi; }
-            } else {
-                if (xi == NGL - 1) { side = 1; j = eta; }
-                else if (xi == 0) { side = 3; j = eta; }
-            }
-            if (side >= 0) {
-                const int4 sd = a.side[(long)e * 4 + side];
-                const int inc = sd.z ? j : NGL - 1 - j;
-                const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
-                const int ms = sd.y;
-                const double db = 0.0;
-                r0 += -ms * fp[0] * J;
-                r1 += -ms * J * fp[NGL] + J * db;
-                r2 += -ms * J * fp[2 * NGL] + J * db;
+            if (ms[pass] != 0) {
+                const int m = ms[pass];
+                r0 += -m * f[pass][0] * J;
+                r1 += -m * J * f[pass][1] + J * db;
+                r2 += -m * J * f[pass][2] + J * db;
             }
         }
         if (a.mode == 2) {
             a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
         } else {
-            const double dt = a.st[ins].dt;
             double q0, q1, q2;
             if (a.mode == 0) {
-                const double g0 = a.rkA * a.gRK[qid] + r0;
-                const double g1 = a.rkA * a.gRK[qid + N2] + r1;
-                const double g2 = a.rkA * a.gRK[qid + 2 * N2] + r2;
+                const double g0 = a.rkA * o0 + r0;
+                const double g1 = a.rkA * o1 + r1;
+                const double g2 = a.rkA * o2 + r2;
                 a.gRK[qid] = g0; a.gRK[qid + N2] = g1; a.gRK[qid + 2 * N2] = g2;
                 q0 = h + a.rkC * dt * g0;
                 q1 = hu + a.rkC * dt * g1;
                 q2 = hv + a.rkC * dt * g2;
             } else {
-                q0 = a.rkA * a.Qtmp[qid] + a.rkB * h + a.rkC * dt * r0;
-                q1 = a.rkA * a.Qtmp[qid + N2] + a.rkB * hu + a.rkC * dt * r1;
-                q2 = a.rkA * a.Qtmp[qid + 2 * N2] + a.rkB * hv + a.rkC * dt * r2;
+                q0 = a.rkA * o0 + a.rkB * h + a.rkC * dt * r0;
+                q1 = a.rkA * o1 + a.rkB * hu + a.rkC * dt * r1;
+                q2 = a.rkA * o2 + a.rkB * hv + a.rkC * dt * r2;
             }
             a.q[qid] = q0; a.q[qid + N2] = q1; a.q[qid + 2 * N2] = q2;
             if (a.lam) lam = node_lambda(a.c, q0, q1, q2);

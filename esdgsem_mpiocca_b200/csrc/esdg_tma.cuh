@@ -1,0 +1,264 @@
+// Bulk-copy (TMA, cp.async.bulk) pipeline helpers for sm_100a and the
+// persistent, double-buffered element kernel built on them.
+//
+// Each CTA walks tiles of NE consecutive elements (tile = blockIdx.x,
+// blockIdx.x + gridDim.x, ...).  One thread issues, per tile, nine 1-D bulk
+// copies global -> shared (q, gRK or Qtmp, Jinv, Bx, By, Y_xi, Y_eta, X_xi,
+// X_eta: all contiguous in the element-major layout) completing on the
+// stage's mbarrier; while the CTA computes tile k the copies of tile k+1 are
+// in flight.  The arithmetic per node is that of k_element (same operands,
+// same order), only the staging differs.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "esdg_kernels.cuh"
+
+namespace esdg {
+
+enum : int { ST_TIMEOUT = 2 };
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// 1-D bulk copy global -> shared; dst, src and bytes are multiples of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Waits for the phase with the given parity; gives up after ~2 s of clock
+// (a copy that never lands), returning false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > 4000000000ll) return false;
+    return true;
+}
+
+template <int NGL>
+struct TmaShape {
+    static constexpr int N2 = NGL * NGL;
+    // elements per tile: ~256 threads, NE*N2 even (16-byte bulk granularity)
+    static constexpr int NE0 = (256 / N2) > 0 ? (256 / N2) : 1;
+    static constexpr int NE = (N2 % 2 == 1 && NE0 % 2 == 1) ? (NE0 > 1 ? NE0 - 1 : 2) : NE0;
+    static constexpr int THREADS = NE * N2;
+    static constexpr int STAGES = 2;
+    static constexpr int QD = NE * 3 * N2;  // doubles of a q-like section
+    static constexpr int ND = NE * N2;      // doubles of a nodal section
+    static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND;
+    // shared layout: [STAGES][stage] | si[ND] | sD[N2] | red[ND] | mbar[STAGES]
+    static constexpr size_t SMEM = sizeof(double) * (STAGES * (size_t)STAGE_DOUBLES + 2 * ND + N2) + 16 * STAGES;
+};
+
+// Issues the bulk copies of tile t into stage buffer sb (one thread).
+template <int NGL>
+__device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double* sb, uint64_t* bar) {
+    using S = TmaShape<NGL>;
+    const int e0 = t * S::NE;
+    const int ne = min(S::NE, a.K - e0);
+    const unsigned qb = (unsigned)(ne * 3 * S::N2 * sizeof(double));
+    const unsigned nb = (unsigned)(ne * S::N2 * sizeof(double));
+    const double* second = (a.mode == 1) ? a.Qtmp : a.gRK;
+    const bool need2 = a.mode != 2;
+    mbar_arrive_expect_tx(bar, qb + (need2 ? qb : 0u) + 7u * nb);
+    const long qo = (long)e0 * 3 * S::N2, no = (long)e0 * S::N2;
+    bulk_g2s(sb, a.q + qo, qb, bar);
+    if (need2) bulk_g2s(sb + S::QD, second + qo, qb, bar);
+    double* nd = sb + 2 * S::QD;
+    bulk_g2s(nd + 0 * S::ND, a.Jinv + no, nb, bar);
+    bulk_g2s(nd + 1 * S::ND, a.Bx + no, nb, bar);
+    bulk_g2s(nd + 2 * S::ND, a.By + no, nb, bar);
+    bulk_g2s(nd + 3 * S::ND, a.Yxi + no, nb, bar);
+    bulk_g2s(nd + 4 * S::ND, a.Yeta + no, nb, bar);
+    bulk_g2s(nd + 5 * S::ND, a.Xxi + no, nb, bar);
+    bulk_g2s(nd + 6 * S::ND, a.Xeta + no, nb, bar);
+}
+
+// Persistent flux-differencing volume term + surface lift + RK update
+// (same operations as k_element), tiles double-buffered through TMA.
+template <int NGL>
+__global__ void __launch_bounds__(TmaShape<NGL>::THREADS, 2) k_element_tma(ElemArgs a, int ntiles) {
+    using S = TmaShape<NGL>;
+    constexpr int N2 = S::N2, NE = S::NE, ST = S::STAGES;
+    extern __shared__ __align__(128) double smem[];
+    double* stage = smem;
+    double* si = smem + ST * S::STAGE_DOUBLES;
+    double* sD = si + S::ND;
+    double* red = sD + N2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(red + S::ND);
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int xi = nd % NGL, eta = nd / NGL;
+    if (tid < N2) sD[tid] = a.D[tid];
+    if (tid == 0)
+        for (int k = 0; k < ST; ++k) mbar_init(&bar[k], 1);
+    __syncthreads();
+    if (tid == 0)
+        for (int k = 0; k < ST; ++k) {
+            const int t = blockIdx.x + k * gridDim.x;
+            if (t < ntiles) tma_issue_tile<NGL>(a, t, stage + k * S::STAGE_DOUBLES, &bar[k]);
+        }
+    const double fg = a.c.fourth_g, hg = a.c.half_g;
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int sidx = it % ST;
+        const unsigned parity = (unsigned)((it / ST) & 1);
+        double* sb = stage + sidx * S::STAGE_DOUBLES;
+        const double* sq = sb;
+        const double* s2 = sb + S::QD;
+        const double* sJ = sb + 2 * S::QD;
+        const double* sBx = sJ + S::ND;
+        const double* sBy = sJ + 2 * S::ND;
+        const double* sYx = sJ + 3 * S::ND;
+        const double* sYe = sJ + 4 * S::ND;
+        const double* sXx = sJ + 5 * S::ND;
+        const double* sXe = sJ + 6 * S::ND;
+        const int e0 = t * NE;
+        const int e = e0 + el;
+        const bool inb = e < a.K;
+        const int ins = inb ? inst_of(a.elem_inst, e) : 0;
+        const bool active = inb && !a.st[ins].done;
+        // face fluxes of this node's sides (global, mostly L2) before the wait
+        double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        int ms[2] = {0, 0};
+        double dt = 0.0;
+        if (active) {
+            if (a.mode != 2) dt = a.st[ins].dt;
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                int side = -1, j = 0;
+                if (pass == 0) {
+                    if (eta == 0) { side = 0; j = xi; }
+                    else if (eta == NGL - 1) { side = 2; j = xi; }
+                } else {
+                    if (xi == NGL - 1) { side = 1; j = eta; }
+                    else if (xi == 0) { side = 3; j = eta; }
+                }
+                if (side >= 0) {
+                    const int4 sd = a.side[(long)e * 4 + side];
+                    const int inc = sd.z ? j : NGL - 1 - j;
+                    const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
+                    ms[pass] = sd.y;
+                    f[pass][0] = fp[0]; f[pass][1] = fp[NGL]; f[pass][2] = fp[2 * NGL];
+                }
+            }
+        }
+        // every thread waits for the tile; a copy that never lands makes the
+        // whole CTA leave together (uniform decision) with an error status
+        // for the host instead of hanging
+        const bool landed = mbar_wait_bounded(&bar[sidx], parity);
+        if (__syncthreads_or(!landed)) {
+            if (tid == 0) atomicExch(&a.st[0].status, ST_TIMEOUT);
+            return;
+        }
+        const int s = el * N2 + nd;          // node slot in nodal sections
+        const int qs = el * 3 * N2 + nd;     // node slot in q sections
+        double h = 0, hu = 0, hv = 0;
+        if (active) {
+            h = sq[qs]; hu = sq[qs + N2]; hv = sq[qs + 2 * N2];
+            si[s] = (h > 0) ? 1.0 / h : 0.0;
+        }
+        __syncthreads();
+        double lam = 0.0;
+        if (active) {
+            const int rb = el * N2 + eta * NGL, cb = el * N2 + xi;
+            const int qrb = el * 3 * N2 + eta * NGL, qcb = el * 3 * N2 + xi;
+            const double ih = si[s], ye = sYe[s], yx = sYx[s], xe = sXe[s], xx = sXx[s];
+            double d1 = 0.0, d2 = 0.0, d3 = 0.0;
+#pragma unroll
+            for (int l = 0; l < NGL; ++l) {
+                const int p = rb + l, pq = qrb + l;
+                const double dl = sD[xi * NGL + l];
+                double f1, f2, f3;
+                two_point_xi(fg, hg, h, hu, hv, ih, sq[pq], sq[pq + N2], sq[pq + 2 * N2], si[p], ye, sYe[p], xe,
+                             sXe[p], f1, f2, f3);
+                d1 += dl * f1; d2 += dl * f2; d3 += dl * f3;
+            }
+#pragma unroll
+            for (int l = 0; l < NGL; ++l) {
+                const int p = cb + l * NGL, pq = qcb + l * NGL;
+                const double dl = sD[eta * NGL + l];
+                double g1, g2, g3;
+                two_point_eta(fg, hg, h, hu, hv, ih, sq[pq], sq[pq + N2], sq[pq + 2 * N2], si[p], yx, sYx[p], xx,
+                              sXx[p], g1, g2, g3);
+                d1 += dl * g1; d2 += dl * g2; d3 += dl * g3;
+            }
+            const double J = sJ[s];
+            double r0 = -J * d1;
+            double r1 = -J * d2 - a.c.g * h * sBx[s];
+            double r2 = -J * d3 - a.c.g * h * sBy[s];
+            const double db = 0.0;
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                if (ms[pass] != 0) {
+                    const int m = ms[pass];
+                    r0 += -m * f[pass][0] * J;
+                    r1 += -m * J * f[pass][1] + J * db;
+                    r2 += -m * J * f[pass][2] + J * db;
+                }
+            }
+            const long qid = (long)e * 3 * N2 + nd;
+            if (a.mode == 2) {
+                a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
+            } else {
+                const double o0 = s2[qs], o1 = s2[qs + N2], o2 = s2[qs + 2 * N2];
+                double q0, q1, q2;
+                if (a.mode == 0) {
+                    const double g0 = a.rkA * o0 + r0;
+                    const double g1 = a.rkA * o1 + r1;
+                    const double g2 = a.rkA * o2 + r2;
+                    a.gRK[qid] = g0; a.gRK[qid + N2] = g1; a.gRK[qid + 2 * N2] = g2;
+                    q0 = h + a.rkC * dt * g0;
+                    q1 = hu + a.rkC * dt * g1;
+                    q2 = hv + a.rkC * dt * g2;
+                } else {
+                    q0 = a.rkA * o0 + a.rkB * h + a.rkC * dt * r0;
+                    q1 = a.rkA * o1 + a.rkB * hu + a.rkC * dt * r1;
+                    q2 = a.rkA * o2 + a.rkB * hv + a.rkC * dt * r2;
+                }
+                a.q[qid] = q0; a.q[qid + N2] = q1; a.q[qid + 2 * N2] = q2;
+                if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
+            }
+        }
+        if (a.lam) block_lambda<NGL, NE>(lam, active, el, nd, e0, a.K, a.elem_inst, a.st, red);
+        __syncthreads();  // stage buffer and si free again
+        if (tid == 0) {
+            const int tn = t + ST * gridDim.x;
+            if (tn < ntiles) {
+                fence_proxy_async_smem();
+                tma_issue_tile<NGL>(a, tn, sb, &bar[sidx]);
+            }
+        }
+    }
+}
+
+}  // namespace esdg

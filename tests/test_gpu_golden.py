@@ -30,3 +30,19 @@ def test_engine_matches_reference_run(name):
         den = np.linalg.norm(b[:, v])
         err = np.linalg.norm(a[:, v] - b[:, v]) / (den if den > 0 else 1.0)
         assert err <= 1e-12, (name, v, err)
+
+
+@pytest.mark.parametrize("name", [n for n in fixtures.names() if "_av_" not in n])
+def test_plain_path_is_bitwise_equal_to_reference(name):
+    """Built without FMA contraction, the engine performs the reference's
+    operations in the reference's order: the plain path (no shock sensor,
+    whose log10/sin come from different math libraries) reproduces the
+    reference's state bit for bit."""
+    prob, q_ref, _ = fixtures.load(name)
+    s = Solver(prob)
+    try:
+        s.run(T=prob.params.T, max_steps=0)
+        q = s.q()
+    finally:
+        s.close()
+    np.testing.assert_array_equal(q, q_ref)
