@@ -226,7 +226,7 @@ def main():
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded curved_lake generator; no dataset exists)",
         "config": workload_config(prob, {"sim_time_reached": t_sim}),
-        "roofline": {"bound": "hbm", "kernel": "k_element<5>", "achieved": ach, "peak": hbm, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "k_element_tma<5>", "achieved": ach, "peak": hbm, "unit": "GB/s",
                      "frac": ach / hbm, "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                      "traffic": traffic,
                      "bytes_per_node": ELEM_BYTES_PER_NODE, "launch_ms": kern["ms"],

@@ -190,37 +190,31 @@ struct ElemShape {
     static constexpr int THREADS = NE * N2;
 };
 
-// Wave-speed maximum of the block's elements, folded into the owning
-// instance's key (okl/DG/FindLambdaMax.okl:17-100 per node; the reduction
-// is a max, so its order does not matter).
-template <int NGL, int NE>
-__device__ __forceinline__ void block_lambda(double lam, bool valid, int el, int nd, int e0, int K,
-                                             const int* elem_inst, DevState* st, double* sred) {
-    constexpr int N2 = NGL * NGL;
-    __syncthreads();
-    sred[el * N2 + nd] = valid ? lam : 0.0;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int cur = -1;
-        double m = 0.0;
-        for (int k = 0; k < NE; ++k) {
-            const int e = e0 + k;
-            if (e >= K) break;
-            const int ins = inst_of(elem_inst, e);
-            double le = 0.0;
-            for (int p = 0; p < N2; ++p) {
-                const double v = sred[k * N2 + p];
-                le = (isnan(v) || v > le) ? v : le;
-            }
-            if (ins != cur) {
-                if (cur >= 0) atomicMax(&st[cur].lam_key, dbl_key(m));
-                cur = ins;
-                m = le;
-            } else {
-                m = (isnan(le) || le > m) ? le : m;
-            }
+// Wave-speed maximum folded into the owning instance's key
+// (okl/DG/FindLambdaMax.okl:17-100 per node; a max, so the reduction order
+// does not matter).  Warp-level and barrier-free: a shuffle reduction and
+// one atomic per warp when all its lanes belong to one instance (always for
+// a single mesh), one atomic per lane otherwise.  Must be called by every
+// thread of the block (THREADS threads, the last warp possibly partial).
+template <int THREADS>
+__device__ __forceinline__ void warp_lambda(double lam, bool valid, int ins, DevState* st) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nl = (warp == (THREADS - 1) / 32 && (THREADS % 32) != 0) ? (THREADS % 32) : 32;
+    const unsigned mask = (nl == 32) ? 0xffffffffu : ((1u << nl) - 1u);
+    const int my = valid ? ins : -1;
+    const int top = __reduce_max_sync(mask, my);
+    if (top < 0) return;  // no valid lane in this warp
+    const int low = -__reduce_max_sync(mask, valid ? -ins : -0x7fffffff);
+    if (low == top) {
+        double v = valid ? lam : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_down_sync(mask, v, off);
+            if (lane + off < nl) v = (isnan(o) || o > v) ? o : v;
         }
-        if (cur >= 0) atomicMax(&st[cur].lam_key, dbl_key(m));
+        if (lane == 0) atomicMax(&st[top].lam_key, dbl_key(v));
+    } else if (valid) {
+        atomicMax(&st[ins].lam_key, dbl_key(lam));
     }
 }
 
@@ -345,7 +339,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
             if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
         }
     }
-    if (a.lam) block_lambda<NGL, NE>(lam, active, el, nd, e0, a.K, a.elem_inst, a.st, sh);
+    if (a.lam) warp_lambda<ElemShape<NGL>::THREADS>(lam, active, ins, a.st);
 }
 
 // Modal energy sensor of one element (okl/ShockCapturing/ShockCapturing.okl:17-234),
@@ -618,7 +612,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av2(ElemArg
             if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
         }
     }
-    if (a.lam) block_lambda<NGL, NE>(lam, active, el, nd, e0, a.K, a.elem_inst, a.st, sF2);
+    if (a.lam) warp_lambda<ElemShape<NGL>::THREADS>(lam, active, ins, a.st);
 }
 
 // Positivity limiter (okl/Positivity/PosPres.okl:17-223), optionally with the
@@ -689,7 +683,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_pospres(int K, cons
         }
         if (lam_flag) lam = node_lambda(c, h, hu, hv);
     }
-    if (lam_flag) block_lambda<NGL, NE>(lam, active, el, nd, e0, K, elem_inst, st, sJ);
+    if (lam_flag) warp_lambda<ElemShape<NGL>::THREADS>(lam, active, ins, st);
 }
 
 // Wave-speed maximum of q (start of the time loop).
@@ -698,18 +692,18 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_lambda(int K, const
                                                                   const int* __restrict__ elem_inst, DevState* st,
                                                                   PhysConst c) {
     constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
-    __shared__ double sred[NE * N2];
     const int tid = threadIdx.x;
     const int el = tid / N2, nd = tid % N2;
     const int e0 = blockIdx.x * NE;
     const int e = e0 + el;
     const bool inb = e < K;
     double lam = 0.0;
+    const int ins = inb ? inst_of(elem_inst, e) : 0;
     if (inb) {
         const long qid = (long)e * 3 * N2 + nd;
         lam = node_lambda(c, q[qid], q[qid + N2], q[qid + 2 * N2]);
     }
-    block_lambda<NGL, NE>(lam, inb, el, nd, e0, K, elem_inst, st, sred);
+    warp_lambda<ElemShape<NGL>::THREADS>(lam, inb, ins, st);
 }
 
 // Step bookkeeping per instance (src/deviceclass.cpp:897-930 and :1130):

@@ -64,6 +64,48 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
     return true;
 }
 
+// Entropy-conservative two-point flux of okl/DG/VolumeKernelFluxDiffV99.okl:17-57,
+// evaluated on raw sums.  Every average there is 0.5*(L+R) and every
+// product of two averages then carries a factor 1/4 or 1/8; scaling by a
+// power of two commutes exactly with IEEE rounding (no subnormals here), so
+//   F1 = (Sa*Shu - Sb*Shv) / 4,
+//   F2 = (Sa*(Shu*Su + P4) - (Sb*Shv)*Su) / 8,
+//   F3 = (Sa*(Shu*Sv) - Sb*(Shv*Sv + P4)) / 8,   P4 = (g*Sh)*Sh - g*Sh2 = 4p,
+// with S* = L+R (u = hu*(1/h), v, h2 = h*h formed once per node, as the
+// reference forms them inside every pair), are the reference's values times
+// 4 resp. 8, bit for bit.  The caller accumulates D*F on the unscaled values
+// and applies 1/4 and 1/8 once per node, which is exact for the same reason.
+// ETA selects G = -a f + b g instead of F = a f - b g.
+template <bool ETA>
+__device__ __forceinline__ void pair_flux_raw(double g, double hL, double huL, double hvL, double uL, double vL,
+                                              double h2L, double aL, double bL, double hR, double huR, double hvR,
+                                              double uR, double vR, double h2R, double aR, double bR, double& X1,
+                                              double& X2, double& X3) {
+    const double Sh = hL + hR;
+    const double Sh2 = h2L + h2R;
+    const double Shu = huL + huR;
+    const double Shv = hvL + hvR;
+    const double Su = uL + uR;
+    const double Sv = vL + vR;
+    const double Sa = aL + aR;
+    const double Sb = bL + bR;
+    const double P4 = g * Sh * Sh - g * Sh2;
+    const double bhv = Sb * Shv;
+    if (!ETA) {
+        X1 = Sa * Shu - bhv;
+        X2 = Sa * (Shu * Su + P4) - bhv * Su;
+        X3 = Sa * (Shu * Sv) - Sb * (Shv * Sv + P4);
+    } else {
+        X1 = -Sa * Shu + bhv;
+        X2 = -Sa * (Shu * Su + P4) + bhv * Su;
+        X3 = -Sa * (Shu * Sv) + Sb * (Shv * Sv + P4);
+    }
+}
+
+#ifndef ESDG_TMA_MIN_BLOCKS
+#define ESDG_TMA_MIN_BLOCKS 2
+#endif
+
 template <int NGL>
 struct TmaShape {
     static constexpr int N2 = NGL * NGL;
@@ -75,8 +117,8 @@ struct TmaShape {
     static constexpr int QD = NE * 3 * N2;  // doubles of a q-like section
     static constexpr int ND = NE * N2;      // doubles of a nodal section
     static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND;
-    // shared layout: [STAGES][stage] | si[ND] | sD[N2] | red[ND] | mbar[STAGES]
-    static constexpr size_t SMEM = sizeof(double) * (STAGES * (size_t)STAGE_DOUBLES + 2 * ND + N2) + 16 * STAGES;
+    // shared layout: [STAGES][stage] | su, sv, sh2 [ND each] | sD[N2] | mbar[STAGES]
+    static constexpr size_t SMEM = sizeof(double) * (STAGES * (size_t)STAGE_DOUBLES + 3 * ND + N2) + 16 * STAGES;
 };
 
 // Issues the bulk copies of tile t into stage buffer sb (one thread).
@@ -106,15 +148,16 @@ __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double*
 // Persistent flux-differencing volume term + surface lift + RK update
 // (same operations as k_element), tiles double-buffered through TMA.
 template <int NGL>
-__global__ void __launch_bounds__(TmaShape<NGL>::THREADS, 2) k_element_tma(ElemArgs a, int ntiles) {
+__global__ void __launch_bounds__(TmaShape<NGL>::THREADS, ESDG_TMA_MIN_BLOCKS) k_element_tma(ElemArgs a, int ntiles) {
     using S = TmaShape<NGL>;
     constexpr int N2 = S::N2, NE = S::NE, ST = S::STAGES;
     extern __shared__ __align__(128) double smem[];
     double* stage = smem;
-    double* si = smem + ST * S::STAGE_DOUBLES;
-    double* sD = si + S::ND;
-    double* red = sD + N2;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(red + S::ND);
+    double* su = smem + ST * S::STAGE_DOUBLES;
+    double* sv = su + S::ND;
+    double* sh2 = sv + S::ND;
+    double* sD = sh2 + S::ND;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sD + N2);
     const int tid = threadIdx.x;
     const int el = tid / N2, nd = tid % N2;
     const int xi = nd % NGL, eta = nd / NGL;
@@ -127,7 +170,6 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, 2) k_element_tma(ElemA
             const int t = blockIdx.x + k * gridDim.x;
             if (t < ntiles) tma_issue_tile<NGL>(a, t, stage + k * S::STAGE_DOUBLES, &bar[k]);
         }
-    const double fg = a.c.fourth_g, hg = a.c.half_g;
     int it = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
         const int sidx = it % ST;
@@ -185,22 +227,27 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, 2) k_element_tma(ElemA
         double h = 0, hu = 0, hv = 0;
         if (active) {
             h = sq[qs]; hu = sq[qs + N2]; hv = sq[qs + 2 * N2];
-            si[s] = (h > 0) ? 1.0 / h : 0.0;
+            const double ih = (h > 0) ? 1.0 / h : 0.0;
+            su[s] = hu * ih;
+            sv[s] = hv * ih;
+            sh2[s] = h * h;
         }
         __syncthreads();
         double lam = 0.0;
         if (active) {
             const int rb = el * N2 + eta * NGL, cb = el * N2 + xi;
             const int qrb = el * 3 * N2 + eta * NGL, qcb = el * 3 * N2 + xi;
-            const double ih = si[s], ye = sYe[s], yx = sYx[s], xe = sXe[s], xx = sXx[s];
+            const double ye = sYe[s], yx = sYx[s], xe = sXe[s], xx = sXx[s];
+            const double uL = su[s], vL = sv[s], h2L = sh2[s];
+            const double g = a.c.g;
             double d1 = 0.0, d2 = 0.0, d3 = 0.0;
 #pragma unroll
             for (int l = 0; l < NGL; ++l) {
                 const int p = rb + l, pq = qrb + l;
                 const double dl = sD[xi * NGL + l];
                 double f1, f2, f3;
-                two_point_xi(fg, hg, h, hu, hv, ih, sq[pq], sq[pq + N2], sq[pq + 2 * N2], si[p], ye, sYe[p], xe,
-                             sXe[p], f1, f2, f3);
+                pair_flux_raw<false>(g, h, hu, hv, uL, vL, h2L, ye, xe, sq[pq], sq[pq + N2], sq[pq + 2 * N2], su[p],
+                                     sv[p], sh2[p], sYe[p], sXe[p], f1, f2, f3);
                 d1 += dl * f1; d2 += dl * f2; d3 += dl * f3;
             }
 #pragma unroll
@@ -208,10 +255,13 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, 2) k_element_tma(ElemA
                 const int p = cb + l * NGL, pq = qcb + l * NGL;
                 const double dl = sD[eta * NGL + l];
                 double g1, g2, g3;
-                two_point_eta(fg, hg, h, hu, hv, ih, sq[pq], sq[pq + N2], sq[pq + 2 * N2], si[p], yx, sYx[p], xx,
-                              sXx[p], g1, g2, g3);
+                pair_flux_raw<true>(g, h, hu, hv, uL, vL, h2L, yx, xx, sq[pq], sq[pq + N2], sq[pq + 2 * N2], su[p],
+                                    sv[p], sh2[p], sYx[p], sXx[p], g1, g2, g3);
                 d1 += dl * g1; d2 += dl * g2; d3 += dl * g3;
             }
+            d1 *= 0.25;
+            d2 *= 0.125;
+            d3 *= 0.125;
             const double J = sJ[s];
             double r0 = -J * d1;
             double r1 = -J * d2 - a.c.g * h * sBx[s];
@@ -249,7 +299,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, 2) k_element_tma(ElemA
                 if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
             }
         }
-        if (a.lam) block_lambda<NGL, NE>(lam, active, el, nd, e0, a.K, a.elem_inst, a.st, red);
+        if (a.lam) warp_lambda<S::THREADS>(lam, active, ins, a.st);
         __syncthreads();  // stage buffer and si free again
         if (tid == 0) {
             const int tn = t + ST * gridDim.x;
