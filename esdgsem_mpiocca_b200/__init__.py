@@ -44,6 +44,7 @@ def _declare(lib):
         "esdg_set_stream": (_I, [_VP, _VP]),
         "esdg_advance": (_I, [_VP, _I, _D, _PD, _PI]),
         "esdg_profile_steps": (_I, [_VP, _I, _PD, _PD]),
+        "esdg_compute_rhs_noalloc": (_I, [_I, _I, _I, _I, _I, _D, _D] + [_VP] * 17 + [_VP, _VP]),
         "esdg_basis": (_I, [_I, _I] + [_PD] * 9),
         "esdg_mesh_cartesian": (_I, [_I, _D, _D, _D, _D, _I, _I, _I, _I, ctypes.POINTER(_VP)]),
         "esdg_mesh_mapped": (_I, [_I, _D, _D, _D, _D, _I, _I, _D, _I, ctypes.c_uint, ctypes.POINTER(_VP)]),

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -957,3 +958,191 @@ int esdg_diagnostics(int K, int N, const double* wGL, const double* Jinv, const 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Right-hand side without any allocation (esdg_compute_rhs_noalloc).
+//
+// For callers that may not allocate device memory themselves: code that runs
+// while a stream is being captured into a CUDA graph, hosts whose memory is
+// owned by their own pool allocator, and serving loops that must not stall
+// on cudaMalloc/cudaFree (both synchronise the device).  They pass their own
+// device buffers for the inputs and the output; the scratch this evaluation
+// needs (packed face/side tables, bathymetry traces, face fluxes, a step
+// state) lives in one file-scope device array of fixed size.
+// ===========================================================================
+namespace esdg {
+
+// 16 MiB of scratch per device, held from library load until process exit.
+constexpr long long kNoAllocScratchDoubles = 1ll << 21;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+struct NoAllocLayout {
+    long long st, err, ftab, side, bL, bR, SP, total;  // offsets in doubles
+};
+
+static NoAllocLayout noalloc_layout(int K, int F, int ngl) {
+    auto up = [](long long v) { return (v + 31) / 32 * 32; };  // 256-byte segments
+    NoAllocLayout L;
+    long long o = 0;
+    L.st = o; o = up(o + (long long)(sizeof(DevState) + 7) / 8);
+    L.err = o; o = up(o + 1);
+    L.ftab = o; o = up(o + 2ll * F);
+    L.side = o; o = up(o + 8ll * K);
+    L.bL = o; o = up(o + (long long)F * ngl);
+    L.bR = o; o = up(o + (long long)F * ngl);
+    L.SP = o; o = up(o + 3ll * F * ngl);
+    L.total = o;
+    return L;
+}
+
+// Packs EdgeData / ElemToEdge / MasterSlave / Orientation into the tables the
+// flux and element kernels read, replacing every out-of-range entry by a safe
+// one and counting it, resets the step state, and gathers the bathymetry
+// traces (okl/GatherEdgeData/CollectEdgeData_Bottom.okl:16-134).
+__global__ void k_noalloc_prepare(int K, int F, int ngl, const int* __restrict__ ED, const int* __restrict__ E2E,
+                                  const int* __restrict__ MS, const int* __restrict__ OR, const double* __restrict__ b,
+                                  int4* ftab, int4* side, double* bL, double* bR, DevState* st, int* err) {
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        DevState z;
+        memset(&z, 0, sizeof z);
+        z.T = 1.0;
+        *st = z;
+    }
+    if (gid < F) {
+        const int* r = ED + gid * 8;
+        int eL = r[0], eR = r[1], sL = r[2], sR = r[3], same = r[4] ? 1 : 0, cpuL = r[5], cpuR = r[6];
+        int bad = 0;
+        if (eL < 0 || eL >= K || sL < 0 || sL > 3 || cpuL != 0) { bad = 1; eL = 0; sL = 0; }
+        if (cpuR == -1) eR = -1;
+        else if (cpuR != 0 || eR < 0 || eR >= K || sR < 0 || sR > 3) { bad = 1; eR = -1; }
+        if (eR < 0) sR = 0;
+        if (bad) atomicAdd(err, 1);
+        ftab[gid] = make_int4(eL, eR, sL | (sR << 2) | (same << 4), 0);
+        const int n2 = ngl * ngl;
+        for (int i = 0; i < ngl; ++i) {
+            const double vl = b[(long)eL * n2 + trace_offset(sL, i, ngl)];
+            bL[gid * ngl + i] = vl;
+            bR[gid * ngl + i] = (eR >= 0) ? b[(long)eR * n2 + trace_offset(sR, i, ngl)] : vl;
+        }
+    }
+    if (gid < 4l * K) {
+        int fc = E2E[gid] - 1, ms = MS[gid], orr = OR[gid];
+        int bad = 0;
+        if (fc < 0 || fc >= F) { bad = 1; fc = 0; }
+        if (ms != 1 && ms != -1) { bad = 1; ms = 1; }
+        if (orr != 0 && orr != 1) { bad = 1; orr = 1; }
+        if (bad) atomicAdd(err, 1);
+        side[gid] = make_int4(fc, ms, orr, 0);
+    }
+}
+
+template <int NGL>
+static void noalloc_launch(int K, int F, int NumFlux, const PhysConst& c, const double* q, const double* Jinv,
+                           const double* Yxi, const double* Yeta, const double* Xxi, const double* Xeta,
+                           const double* Bx, const double* By, const double* D, const double* nx, const double* ny,
+                           const double* scal, double* base, const NoAllocLayout& L, double* Qt, cudaStream_t s) {
+    DevState* st = reinterpret_cast<DevState*>(base + L.st);
+    FaceArgs fa{F, reinterpret_cast<const int4*>(base + L.ftab), q, nx, ny, scal, base + L.bL, base + L.bR,
+                base + L.SP, nullptr, nullptr, nullptr, st, c};
+    const long nfn = (long)F * NGL;
+    const int fb = (int)((nfn + 255) / 256);
+    if (NumFlux == 0) k_face_flux<NGL, 0, false><<<fb, 256, 0, s>>>(fa);
+    else if (NumFlux == 2) k_face_flux<NGL, 2, false><<<fb, 256, 0, s>>>(fa);
+    else k_face_flux<NGL, 3, false><<<fb, 256, 0, s>>>(fa);
+    ElemArgs ea;
+    memset(&ea, 0, sizeof ea);
+    ea.K = K; ea.Jinv = Jinv; ea.Yxi = Yxi; ea.Yeta = Yeta; ea.Xxi = Xxi; ea.Xeta = Xeta; ea.Bx = Bx; ea.By = By;
+    ea.D = D; ea.SP = base + L.SP; ea.side = reinterpret_cast<const int4*>(base + L.side);
+    ea.q = const_cast<double*>(q); ea.Qt = Qt; ea.st = st; ea.mode = 2; ea.c = c;
+    using S = ElemShape<NGL>;
+    k_element<NGL><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, s>>>(ea);
+}
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[64] = {nullptr};
+
+}  // namespace esdg
+
+extern "C" int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES, double g_const, double PosPresTOL,
+                                        const double* q, const double* Jinv, const double* y_xi, const double* y_eta,
+                                        const double* x_xi, const double* x_eta, const double* Bx, const double* By,
+                                        const double* b, const double* Dmat, const double* nx, const double* ny,
+                                        const double* scal, const int* EdgeData, const int* ElemToEdge,
+                                        const int* ElemEdgeMasterSlave, const int* ElemEdgeOrientation, double* Qt,
+                                        void* stream) {
+    using namespace esdg;
+    if (N < 1 || N > 7) { g_create_error = "compute_rhs_noalloc: N must be in 1..7"; return ESDG_E_UNSUPPORTED; }
+    if (NumFlux != 0 && NumFlux != 2 && NumFlux != 3) {
+        g_create_error = "compute_rhs_noalloc: NumFlux must be 0, 2 or 3";
+        return ESDG_E_UNSUPPORTED;
+    }
+    if (K <= 0 || F <= 0 || !q || !Jinv || !y_xi || !y_eta || !x_xi || !x_eta || !Bx || !By || !b || !Dmat || !nx ||
+        !ny || !scal || !EdgeData || !ElemToEdge || !ElemEdgeMasterSlave || !ElemEdgeOrientation || !Qt) {
+        g_create_error = "compute_rhs_noalloc: sizes must be positive and every array given";
+        return ESDG_E_ARG;
+    }
+    const int ngl = N + 1;
+    const NoAllocLayout L = noalloc_layout(K, F, ngl);
+    if (L.total > kNoAllocScratchDoubles) {
+        g_create_error = "compute_rhs_noalloc: mesh needs " + std::to_string(L.total) +
+                         " doubles of scratch, the fixed maximum is " + std::to_string(kNoAllocScratchDoubles) +
+                         " (about 5*Nfaces*(N+1) + 8*Nelem)";
+        return ESDG_E_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        g_create_error = std::string("compute_rhs_noalloc: cudaGetDevice: ") + cudaGetErrorString(e);
+        return ESDG_E_CUDA;
+    }
+    double* base = nullptr;
+    {
+        // the device address of the scratch array, looked up once per device
+        // (with that device current) on the first call
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                g_create_error = std::string("compute_rhs_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                return ESDG_E_CUDA;
+            }
+            g_noalloc_ptr[dev] = static_cast<double*>(p);
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int* err = reinterpret_cast<int*>(base + L.err);
+    e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e != cudaSuccess) { g_create_error = std::string("compute_rhs_noalloc: ") + cudaGetErrorString(e); return ESDG_E_CUDA; }
+    const long np = std::max<long>(F, 4l * K);
+    k_noalloc_prepare<<<(int)((np + 255) / 256), 256, 0, s>>>(
+        K, F, ngl, EdgeData, ElemToEdge, ElemEdgeMasterSlave, ElemEdgeOrientation, b,
+        reinterpret_cast<int4*>(base + L.ftab), reinterpret_cast<int4*>(base + L.side), base + L.bL, base + L.bR,
+        reinterpret_cast<DevState*>(base + L.st), err);
+    PhysConst c;
+    c.g = g_const; c.half_g = 0.5 * g_const; c.fourth_g = 0.25 * g_const;
+    c.geomFace = 1.0 / (2.0 / (N * (N + 1.0)));
+    c.PosPresTOL = PosPresTOL; c.eps0 = 0; c.sigmaMin = 0; c.sigmaMax = 0; c.ZeroTOL = std::pow(10.0, -5); c.ES = ES;
+    switch (ngl) {
+        case 2: noalloc_launch<2>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+        case 3: noalloc_launch<3>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+        case 4: noalloc_launch<4>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+        case 5: noalloc_launch<5>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+        case 6: noalloc_launch<6>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+        case 7: noalloc_launch<7>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+        default: noalloc_launch<8>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { g_create_error = std::string("compute_rhs_noalloc: launch: ") + cudaGetErrorString(e); return ESDG_E_CUDA; }
+    int nerr = 0;
+    e = cudaMemcpyAsync(&nerr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { g_create_error = std::string("compute_rhs_noalloc: ") + cudaGetErrorString(e); return ESDG_E_CUDA; }
+    if (nerr) {
+        g_create_error = "compute_rhs_noalloc: " + std::to_string(nerr) + " connectivity entries out of range";
+        return ESDG_E_ARG;
+    }
+    return ESDG_OK;
+}
