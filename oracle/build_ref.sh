@@ -18,3 +18,21 @@ for f in "$REF"/src/*.cpp "$REF"/main.cpp "$HERE"/ref_shim/occa_shim.cpp; do
 done
 g++ -o "$OUT/esdg_ref" "$OUT"/obj/*.o -ldl
 echo "$OUT/esdg_ref"
+
+# The reference's main.cpp and host sources (everything but its deviceclass)
+# linked against the B200 engine through include/dropin/deviceclass.h: the
+# drop-in boundary exercised by the reference's own driver.
+if [ "$1" = "dropin" ]; then
+  REPO=$(cd "$HERE/.." && pwd)
+  LIB="$REPO/esdgsem_mpiocca_b200"
+  mkdir -p "$OUT/dropin_obj"
+  DFLAGS="-O2 -ffp-contract=off -w -std=gnu++14 -I$REPO/include/dropin -I$REPO/include -I$HERE/ref_shim -I$REF/include"
+  for f in "$REF"/src/*.cpp "$REF"/main.cpp; do
+    case "$f" in *deviceclass.cpp) continue;; esac
+    o="$OUT/dropin_obj/$(basename "$f" .cpp).o"
+    g++ $DFLAGS -Ddfloat=double -Ddfloat4=double4 -DMPI_DFLOAT=MPI_DOUBLE '-DdfloatString="double"' \
+        '-Ddfloat4String="double4"' -c "$f" -o "$o"
+  done
+  g++ -o "$OUT/esdg_dropin" "$OUT"/dropin_obj/*.o -L"$LIB" -lesdg_b200 -Wl,-rpath,'$ORIGIN/../../esdgsem_mpiocca_b200'
+  echo "$OUT/esdg_dropin"
+fi

@@ -159,6 +159,46 @@ CASES = {
     "walls_ssp3_N2": lambda: case_ssp_walls(),
 }
 
+
+
+# ---------------------------------------------------------------------------
+# Printed diagnostics of the reference's own driver on a native test case,
+# for the drop-in test (the reference's main.cpp linked against the engine).
+DROPIN_CASES = {
+    # Testcase 20: Cartesian dam break (h = 10 | 5), b = 0, solid walls
+    "dropin_tc20_nf0": dict(N=3, T=0.02, NumFlux=0, Testcase=20, cart=(-5.0, 5.0, -5.0, 5.0, 20, 20, 0, 0)),
+    "dropin_tc20_nf3_ssp": dict(N=4, T=0.02, NumFlux=3, Testcase=20, rkOrder=3, rkSSP=1,
+                                cart=(-5.0, 5.0, -5.0, 5.0, 12, 10, 0, 0)),
+}
+
+
+def dropin_params(spec):
+    p = host.Params(N=spec["N"], CFL=0.4, T=spec["T"], NumFlux=spec["NumFlux"], Testcase=spec["Testcase"],
+                    rkOrder=spec.get("rkOrder", 4), rkSSP=spec.get("rkSSP", 0))
+    return p
+
+
+def diag_lines(stdout):
+    keys = ("Entropydifference is", "relative Entropydifference", "Mass difference is", "relative mass difference",
+            "L2Error[", "LinfError[")
+    return [ln.strip() for ln in stdout.splitlines() if ln.strip().startswith(keys)]
+
+
+def make_dropin(name):
+    spec = DROPIN_CASES[name]
+    p = dropin_params(spec)
+    out = run_ref.run(name, p, cartesian=spec["cart"])
+    rec = {"spec": spec, "params": {k: getattr(p, k) for k in vars(p)}, "diagnostics": diag_lines(out["stdout"]),
+           "input_dat": open(os.path.join(ROOT, "oracle", "_ref", "runs", name, "input.dat")).read(),
+           "cartesian_dat": open(os.path.join(ROOT, "oracle", "_ref", "runs", name, "Cartesian.dat")).read()}
+    with open(os.path.join(OUT, f"{name}.json"), "w") as f:
+        json.dump(rec, f, indent=1)
+    print(name, rec["diagnostics"])
+
+
+for _n in DROPIN_CASES:
+    CASES[_n] = (lambda n: (lambda: make_dropin(n)))(_n)
+
 if __name__ == "__main__":
     if not run_ref.available():
         sys.exit("the reference tree is not available here")

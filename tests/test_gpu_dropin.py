@@ -1,0 +1,44 @@
+"""The reference's own driver on the B200 engine (GPU).
+
+oracle/_ref/esdg_dropin is the reference's main.cpp and host sources (all
+but its deviceclass) compiled where they lie and linked against
+libesdg_b200.so through include/dropin/deviceclass.h (built by
+`oracle/build_ref.sh dropin` in a container that has the reference tree;
+the binary travels with the repository, the reference tree does not).  Run
+on a native test case (Testcase 20, Cartesian dam break, solid walls), its
+printed end-of-run diagnostics -- L2 and Linf errors, mass and entropy
+changes, printed with 17 significant digits (main.cpp:77) -- must equal,
+character for character, those of the reference program itself recorded in
+tests/golden/dropin_*.json.
+"""
+import glob
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "oracle", "_ref", "esdg_dropin")
+CASES = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "dropin_*.json")))
+
+pytestmark = pytest.mark.gpu
+
+
+def diag_lines(stdout):
+    keys = ("Entropydifference is", "relative Entropydifference", "Mass difference is", "relative mass difference",
+            "L2Error[", "LinfError[")
+    return [ln.strip() for ln in stdout.splitlines() if ln.strip().startswith(keys)]
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="drop-in driver not built (oracle/build_ref.sh dropin)")
+@pytest.mark.parametrize("case", CASES, ids=[os.path.basename(c)[:-5] for c in CASES])
+def test_reference_driver_on_engine_prints_reference_results(case, tmp_path):
+    rec = json.load(open(case))
+    (tmp_path / "input.dat").write_text(rec["input_dat"])
+    (tmp_path / "Cartesian.dat").write_text(rec["cartesian_dat"])
+    p = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {EXE} CUDA"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    got = diag_lines(p.stdout)
+    assert got == rec["diagnostics"], (got, rec["diagnostics"])
