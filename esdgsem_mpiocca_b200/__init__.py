@@ -57,6 +57,19 @@ def _declare(lib):
         "esdg_element_sizes": (_I, [_I, _I, _PD, _PD, _PD, _PD]),
         "esdg_rk_coefficients": (_I, [_I, _I, _PD, _PD, _PD, _PI]),
         "esdg_diagnostics": (_I, [_I, _I, _PD, _PD, _PD, _PD, _PD, _D, _PD, _PD, _PD, _PD]),
+        "esdg_ensemble_create": (_I, [_I, _I, _I, _I, _I, _I, _I, _D, _D, _I, _D, _D, _D, _I, _I, _I,
+                                      ctypes.POINTER(_VP)]),
+        "esdg_ensemble_add": (_I, [_VP, _I, _I] + [_PD] * 13 + [_PI] * 4 + [_D, _I, _D, _D, _D, _PI]),
+        "esdg_ensemble_remove": (_I, [_VP, _I]),
+        "esdg_ensemble_advance": (_I, [_VP, _I]),
+        "esdg_ensemble_status": (_I, [_VP, _I, _PD, _PI, _PI, _PI]),
+        "esdg_ensemble_copy_q": (_I, [_VP, _I, _PD]),
+        "esdg_ensemble_free_capacity": (_I, [_VP, _PI, _PI, _PI]),
+        "esdg_ensemble_bytes": (ctypes.c_longlong, [_VP]),
+        "esdg_ensemble_kernel_launches": (ctypes.c_longlong, [_VP]),
+        "esdg_ensemble_set_stream": (_I, [_VP, _VP]),
+        "esdg_ensemble_last_error": (ctypes.c_char_p, [_VP]),
+        "esdg_ensemble_destroy": (_I, [_VP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

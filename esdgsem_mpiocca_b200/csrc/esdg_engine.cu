@@ -84,6 +84,7 @@ class Engine {
     DevState* st = nullptr;
     DevState* st_host = nullptr;  // pinned mirror for polling
     int* elem_inst = nullptr;     // null: one instance
+    int I = 1;                    // step-state entries (instances, arena: + one retired slot)
 
     // step graph
     cudaGraphExec_t graph = nullptr;
@@ -177,7 +178,7 @@ class Engine {
                 (r = alloc(&GX, nn * 2)) || (r = alloc(&GY, nn * 2)) || (r = alloc(&VP, (size_t)K)))
                 return r;
         }
-        if ((r = alloc(&st, (size_t)1))) return r;
+        if ((r = alloc(&st, (size_t)I))) return r;
         cudaError_t e = cudaMallocHost(&st_host, sizeof(DevState));
         if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         // the zero fills ran on the legacy stream; order them before any
@@ -388,7 +389,7 @@ class Engine {
     template <int NGL>
     void launch_step() {
         if (AV) launch_shock<NGL>();
-        k_step_begin<<<1, 32, 0, stream>>>(1, st, ngl, AV);
+        k_step_begin<<<(I + 127) / 128, 128, 0, stream>>>(I, st, ngl, AV);
         ++launches;
         if (rkSSP) {
             // o_Qtmp.copyFrom(o_q) (src/deviceclass.cpp:933-936)
@@ -396,7 +397,7 @@ class Engine {
         }
         for (int s = 0; s < gStages; ++s)
             launch_stage<NGL>(rkSSP ? 1 : 0, gA[s], gB[s], gC[s], s == gStages - 1, s > 0);
-        k_step_end<<<1, 32, 0, stream>>>(1, st);
+        k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
         ++launches;
     }
 
@@ -535,7 +536,7 @@ class Engine {
     template <int NGL>
     void launch_step_profiled(double* face_ms, double* elem_ms) {
         if (AV) launch_shock<NGL>();
-        k_step_begin<<<1, 32, 0, stream>>>(1, st, ngl, AV);
+        k_step_begin<<<(I + 127) / 128, 128, 0, stream>>>(I, st, ngl, AV);
         ++launches;
         if (rkSSP)
             cudaMemcpyAsync(Qtmp, q, (size_t)K * ngl * ngl * 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream);
@@ -571,7 +572,7 @@ class Engine {
             *face_ms += a;
             *elem_ms += b;
         }
-        k_step_end<<<1, 32, 0, stream>>>(1, st);
+        k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
         ++launches;
     }
 
@@ -1146,3 +1147,5 @@ extern "C" int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES
     }
     return ESDG_OK;
 }
+
+#include "esdg_arena.cuh"
