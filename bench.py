@@ -163,7 +163,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="curved_lake", choices=["curved_lake", "ensemble"],
+                    help="curved_lake: the headline single-mesh workload; ensemble: 256 seeded tsunami "
+                         "members batched vs one at a time")
+    ap.add_argument("--members", type=int, default=256)
     args = ap.parse_args()
+    if args.workload == "ensemble":
+        return ensemble_bench(args)
     ws, rank, local = dist_env()
     args.warmup = max(args.warmup, 3)
 
@@ -288,6 +294,93 @@ def e2e_run(s, prob, stream, steps, dist, ws):
     return {"value": ws * prob.dofs() * STAGES * steps / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": qh.numel() * 8 / steps, "d2h_bytes_per_step": qo.numel() * 8 / steps,
             "calls": "esdg_copy_q_from_host + esdg_dg_timeloop + esdg_copy_q_to_host"}
+
+
+def member_sizes(seeds):
+    """(K, F) of each tsunami member without building it (the size is the
+    first draw of the member's generator)."""
+    from esdgsem_mpiocca_b200.problems import TSUNAMI_SIZES
+    out = []
+    for s in seeds:
+        nel = int(np.random.default_rng(10_000 + s).choice(TSUNAMI_SIZES))
+        out.append((nel * nel, 2 * nel * (nel + 1)))
+    return out
+
+
+def ensemble_bench(args):
+    """Config 4: 256 tsunami members (N=3, K in {64..256}^2, 500 steps each,
+    artificial viscosity with the modal sensor) advanced in one arena, vs the
+    same kind of members solved one at a time by the single-mesh engine."""
+    import torch
+    from esdgsem_mpiocca_b200 import problems
+    from esdgsem_mpiocca_b200.deviceclass import Solver
+    from esdgsem_mpiocca_b200.ensemble import Ensemble
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    steps = args.steps if args.steps != 400 else 500
+    seeds = list(range(rank * args.members, (rank + 1) * args.members))
+    sizes = member_sizes(seeds)
+    Kc, Fc = sum(k for k, _ in sizes), sum(f for _, f in sizes)
+    p0 = problems.tsunami_member(seeds[0], steps=steps, sizes=(8,))  # parameters only
+    ens = Ensemble(3, len(seeds), Kc, Fc, NumFlux=p0.params.NumFlux, g_const=p0.params.g_const,
+                   PosPresTOL=p0.params.PosPresTOL, ArtificialViscosity=p0.params.ArtificialViscosity,
+                   epsilon_0=p0.params.epsilon_0, sigma_max=p0.params.sigma_max, sigma_min=p0.params.sigma_min)
+    t0 = time.perf_counter()
+    dofs = 0
+    ids = []
+    for sd in seeds:
+        pr = problems.tsunami_member(sd, steps=steps)
+        ids.append(ens.add(pr, T=1e9, max_steps=steps))
+        dofs += pr.dofs()
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    ens.set_stream(stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    launches0 = ens.kernel_launches()
+    with Clocks(local) as ck:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            ens.advance(steps)   # every member runs exactly `steps` steps
+            e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    done = all(ens.status(i)["done"] or ens.status(i)["steps"] == steps for i in ids)
+    bad = [i for i in ids if ens.status(i)["status"] != 0]
+    batched = dofs * STAGES * steps / (ms / 1e3)
+    launches = ens.kernel_launches() - launches0
+    ens.close()
+    # one at a time: members of every size, each alone on the GPU
+    alone_seeds = seeds[: min(len(seeds), 10)]
+    adofs, ams = 0, 0.0
+    for sd in alone_seeds:
+        pr = problems.tsunami_member(sd, steps=steps)
+        s = Solver(pr, device_id=local)
+        st = torch.cuda.Stream()
+        s.dc.set_stream(st.cuda_stream)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            a0.record(st)
+            s.run(T=1e9, max_steps=steps)
+            a1.record(st)
+        torch.cuda.synchronize()
+        ams += a0.elapsed_time(a1)
+        adofs += pr.dofs()
+        s.close()
+    alone = adofs * STAGES * steps / (ams / 1e3)
+    line = {"metric": METRIC, "value": batched * ws, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": 0,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded tsunami members: shelf, seamounts, Okada uplift)",
+            "config": {"workload": f"ensemble of {len(seeds)} tsunami members, N=3, K in {{64..256}}^2 on 2000 km "
+                                   f"squares, {steps} LS-RK4 steps each, artificial viscosity (modal sensor)",
+                       "members": len(seeds), "nodes": dofs, "setup_s": setup_s, "all_done": bool(done),
+                       "members_with_error": len(bad)},
+            "one_at_a_time": {"value": alone, "unit": UNIT, "members": len(alone_seeds),
+                              "ratio_batched_over_alone": batched / alone},
+            "gpu_launches": int(launches), "clocks": ck.result}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 def reference_arm(args, ws, rank):

@@ -86,3 +86,43 @@ def dam_break(N=4, nel=256, seed=0, steps=2000, NumFlux=0, CFL=0.4, AV=1, eps0=N
     n2 = (N + 1) ** 2
     return make_problem(p, m, b, _state(h, K=m.K, n2=n2),
                         {"name": "dam_break", "nel": nel, "seed": seed, "radius": r0, "centre": (cx, cy)})
+
+
+TSUNAMI_SIZES = (64, 96, 128, 192, 256)
+
+
+def tsunami_member(seed, N=3, steps=500, sizes=TSUNAMI_SIZES, AV=1, L=2.0e6, NumFlux=0, CFL=0.4,
+                   eps0=2.0e4, sigma_min=-7.0, sigma_max=-3.0) -> Problem:
+    """One member of the seeded tsunami ensemble: a K x K Cartesian mesh
+    (K drawn from `sizes`) on an L x L square (metres, walls), a shelf 4000 m
+    deep offshore rising linearly to 50 m over the last 200 km, 0-5 Gaussian
+    seamounts, and the Okada uplift of a fault drawn from the seed (length
+    50-400 km, width 20-150 km, top depth 5-30 km, dip 5-30 deg, strike 0-360
+    deg, slip 1-15 m, thrust rake 90 deg) added to the sea surface at rest."""
+    from . import okada
+    rng = np.random.default_rng(10_000 + seed)
+    nel = int(rng.choice(sizes))
+    p = Params(N=N, CFL=CFL, DFL=0.1, T=1.0e9, g_const=9.81, NumFlux=NumFlux, ES=1, rkOrder=4, rkSSP=0,
+               ArtificialViscosity=AV, epsilon_0=eps0, sigma_min=sigma_min, sigma_max=sigma_max, MaxSteps=steps,
+               PosPresTOL=1e-4)
+    m = mesh_cartesian(N, 0.0, L, 0.0, L, nel, nel)
+    x, y = m.x, m.y
+    shelf0 = L - 200.0e3
+    depth = np.where(x < shelf0, 4000.0, 4000.0 - (4000.0 - 50.0) * (x - shelf0) / 200.0e3)
+    b = -depth
+    for _ in range(int(rng.integers(0, 6))):
+        hgt = rng.uniform(500.0, 3000.0)
+        w = rng.uniform(20.0e3, 80.0e3)
+        cx, cy = rng.uniform(0.1 * L, shelf0), rng.uniform(0.1 * L, 0.9 * L)
+        b = b + hgt * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (w * w))
+    b = np.minimum(b, -50.0)
+    f = okada.Fault(x0=rng.uniform(0.2 * L, 0.7 * L), y0=rng.uniform(0.2 * L, 0.8 * L),
+                    depth=rng.uniform(5.0e3, 30.0e3), length=rng.uniform(50.0e3, 400.0e3),
+                    width=rng.uniform(20.0e3, 150.0e3), strike=rng.uniform(0.0, 360.0), rake=90.0,
+                    dip=rng.uniform(5.0, 30.0), slip=rng.uniform(1.0, 15.0))
+    eta = okada.uplift_cartesian(x, y, f)
+    h = -b + eta
+    n2 = (N + 1) ** 2
+    return make_problem(p, m, b, _state(h, K=m.K, n2=n2),
+                        {"name": "tsunami_member", "seed": seed, "nel": nel, "fault": vars(f),
+                         "max_uplift": float(np.abs(eta).max())})

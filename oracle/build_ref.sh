@@ -18,6 +18,9 @@ for f in "$REF"/src/*.cpp "$REF"/main.cpp "$HERE"/ref_shim/occa_shim.cpp; do
 done
 g++ -o "$OUT/esdg_ref" "$OUT"/obj/*.o -ldl
 echo "$OUT/esdg_ref"
+# the reference's Okada routine alone, on points from a file
+g++ $FLAGS -Ddfloat=double -Ddfloat4=double4 -DMPI_DFLOAT=MPI_DOUBLE '-DdfloatString="double"' \
+    '-Ddfloat4String="double4"' -o "$OUT/okada_driver" "$HERE/ref_shim/okada_driver.cpp" "$OUT/obj/okada.o"
 
 # The reference's main.cpp and host sources (everything but its deviceclass)
 # linked against the B200 engine through include/dropin/deviceclass.h: the

@@ -15,7 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.npz")))
+    """Solver fixtures (state after a reference run)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.npz"))
+                  if not os.path.basename(p).startswith("okada"))
 
 
 def load(name):

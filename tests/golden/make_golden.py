@@ -199,6 +199,31 @@ def make_dropin(name):
 for _n in DROPIN_CASES:
     CASES[_n] = (lambda n: (lambda: make_dropin(n)))(_n)
 
+
+# ---------------------------------------------------------------------------
+# The reference's Okada routine (src/okada.cpp) on a lon/lat grid around the
+# epicentre of its shipped fault file data/indianOceanFault1.txt.
+def make_okada(name="okada_fault1"):
+    import subprocess
+    import tempfile
+    R = 6.378e6
+    lon = np.linspace(94.57 - 2.5, 94.57 + 2.5, 121)
+    lat = np.linspace(3.83 - 1.5, 3.83 + 1.5, 73)
+    LO, LA = np.meshgrid(lon, lat)
+    x = (LO * R * np.pi / 180 / 1000).ravel()
+    y = (R * np.arcsinh(np.tan(LA * np.pi / 180)) / 1000).ravel()
+    d = tempfile.mkdtemp()
+    os.symlink(os.path.join(run_ref.REF, "data"), os.path.join(d, "data"))
+    np.concatenate([[x.size], x, y]).astype(np.float64).tofile(os.path.join(d, "pts.bin"))
+    subprocess.run([os.path.join(ROOT, "oracle", "_ref", "okada_driver"), "pts.bin", "out.bin"], cwd=d, check=True)
+    uplift = np.fromfile(os.path.join(d, "out.bin"))
+    fault = [float(v) for v in open(os.path.join(run_ref.REF, "data", "indianOceanFault1.txt")).read().split()]
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), x_km=x, y_km=y, uplift_km=uplift, fault=np.array(fault))
+    print(name, "points", x.size, "nonzero", int((uplift != 0).sum()))
+
+
+CASES["okada_fault1"] = make_okada
+
 if __name__ == "__main__":
     if not run_ref.available():
         sys.exit("the reference tree is not available here")
