@@ -70,6 +70,18 @@ def _declare(lib):
         "esdg_ensemble_set_stream": (_I, [_VP, _VP]),
         "esdg_ensemble_last_error": (ctypes.c_char_p, [_VP]),
         "esdg_ensemble_destroy": (_I, [_VP]),
+        "esdg_state_pointers": (_I, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+        "esdg_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),
+        "esdg_indicator_stats": (_I, [_VP, ctypes.POINTER(ctypes.c_ulonglong), _I]),
+        "esdg_ensemble_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),
+        "esdg_ensemble_indicator_stats": (_I, [_VP, ctypes.POINTER(ctypes.c_ulonglong), _I]),
+        "esdg_mlp_layout": (_I, [_I, _PI]),
+        "esdg_mlp_features": (_I, [_I, _I, _VP, _VP, _VP, _D, _VP, _VP, _VP, _VP]),
+        "esdg_mlp_cast": (_I, [_I, _VP, _VP, _VP]),
+        "esdg_mlp_forward": (_I, [_I, _I, _VP, _VP, _VP, _VP, _I, _VP]),
+        "esdg_mlp_backward": (_I, [_I, _I, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
+        "esdg_mlp_adam": (_I, [_I, _I, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_float, ctypes.c_float,
+                               ctypes.c_float, ctypes.c_float, _I, _VP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -99,6 +99,7 @@ class Arena : public Engine {
             (r = h2d(Vinv, B.VdmInv.data(), B.VdmInv.size(), "Vinv")) ||
             (r = h2d(GLw, B.wGL.data(), B.wGL.size(), "GLw")))
             return r;
+        Vinv_h = B.VdmInv;
         copied = true;
         if ((r = build(1, NumFlux_, rkSSP_, AV_, PP_, 0, 0))) return r;
         double A[8], Bc[8], C[8];
@@ -357,6 +358,18 @@ int esdg_ensemble_set_stream(esdg_ensemble* en, void* cuda_stream) {
     cudaSetDevice(en->a.device);
     en->a.stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : en->a.own_stream;
     return en->a.capture_step_graph();
+}
+
+int esdg_ensemble_set_indicator(esdg_ensemble* en, int mode, const float* params, int nparams, float margin) {
+    if (!en) return ESDG_E_ARG;
+    cudaSetDevice(en->a.device);
+    return en->a.set_indicator(mode, params, nparams, margin);
+}
+
+int esdg_ensemble_indicator_stats(esdg_ensemble* en, unsigned long long* counts4, int reset) {
+    if (!en || !counts4) return ESDG_E_ARG;
+    cudaSetDevice(en->a.device);
+    return en->a.indicator_stats(counts4, reset);
 }
 
 const char* esdg_ensemble_last_error(const esdg_ensemble* en) {

@@ -28,6 +28,7 @@
 #include "../../include/esdg_b200.h"
 #include "esdg_kernels.cuh"
 #include "esdg_tma.cuh"
+#include "esdg_indicator.cuh"
 #include "esdg_setup.hpp"
 
 namespace esdg {
@@ -55,6 +56,49 @@ __global__ void k_collect_bottom_impl(int F, int ngl, const int* ED, const doubl
     br[gid] = vr;
 }
 
+// Smallest and largest eigenvalue of V^T V (V n x n, row-major) by cyclic
+// Jacobi rotations (Golub & Van Loan, Matrix Computations, sec. 8.5).
+static void gram_extremes(const std::vector<double>& V, int n, double* lo, double* hi) {
+    std::vector<double> A((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < n; ++k) acc += V[(size_t)k * n + i] * V[(size_t)k * n + j];
+            A[(size_t)i * n + j] = acc;
+        }
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        double off = 0.0;
+        for (int p = 0; p < n; ++p)
+            for (int q = p + 1; q < n; ++q) off += A[(size_t)p * n + q] * A[(size_t)p * n + q];
+        if (off < 1e-30) break;
+        for (int p = 0; p < n; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[(size_t)p * n + q];
+                if (apq == 0.0) continue;
+                const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; ++k) {  // A <- J^T A J
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - sn * akq;
+                    A[(size_t)k * n + q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - sn * aqk;
+                    A[(size_t)q * n + k] = sn * apk + c * aqk;
+                }
+            }
+    }
+    double mn = A[0], mx = A[0];
+    for (int i = 1; i < n; ++i) {
+        mn = std::min(mn, A[(size_t)i * n + i]);
+        mx = std::max(mx, A[(size_t)i * n + i]);
+    }
+    *lo = mn;
+    *hi = mx;
+}
 
 class Engine {
   public:
@@ -85,6 +129,21 @@ class Engine {
     DevState* st_host = nullptr;  // pinned mirror for polling
     int* elem_inst = nullptr;     // null: one instance
     int I = 1;                    // step-state entries (instances, arena: + one retired slot)
+
+    // Troubled-cell indicator of the artificial-viscosity path: 0 the modal
+    // sensor and the viscous terms on every element (the reference's path);
+    // 1 the modal sensor with the active set (viscous terms only on flagged
+    // elements, same numbers); 2 the learned indicator with the active set.
+    int indicator = 0;
+    float* mlpP = nullptr;
+    __nv_bfloat16* mlpPb = nullptr;
+    float ind_margin = 0.5f;
+    double ind_emin = 0.0, ind_emax = 0.0;
+    int* act = nullptr;                       // [K + 1]: flags, then the list length
+    int* alist = nullptr;                     // [K] flagged elements of the stage
+    unsigned long long* ind_stats = nullptr;  // [4] decision counts
+    std::vector<double> Vinv_h;
+    int list_grid = 0;                        // persistent grid of the list kernels
 
     // step graph
     cudaGraphExec_t graph = nullptr;
@@ -125,6 +184,8 @@ class Engine {
         bytes = 0;
         if (st_host) { cudaFreeHost(st_host); st_host = nullptr; }
         q = gRK = Qt = Qtmp = nullptr;
+        mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr;
+        indicator = 0;
         inited = copied = built = false;
     }
 
@@ -201,7 +262,7 @@ class Engine {
              const double* yxi_h, const double* yeta_h, const double* xxi_h, const double* xeta_h, const double* b_h,
              const double* Bx_h, const double* By_h, const double* D_h, const double* Ds_h, const double* Dh_h,
              const double* J_h, const double* x_h, const double* y_h, const double* q_h, const double* Es_h,
-             const double* gRK_h, const double* Qt_h, const double* Vinv_h, const int* MS_h, const int* OR_h,
+             const double* gRK_h, const double* Qt_h, const double* Vinv_h_, const int* MS_h, const int* OR_h,
              const int* E2E_h, const int* ED_h, const int* ER_h) {
         if (!inited) return fail(ESDG_E_ARG, "copyDeviceVariables before initDeviceVariables");
         if (Nelem != K) return fail(ESDG_E_ARG, "Nelem differs from initDeviceVariables");
@@ -241,7 +302,7 @@ class Engine {
             (r = h2d(Xeta, xeta_h, nn, "x_eta")) || (r = h2d(B, b_h, nn, "b")) || (r = h2d(Bx, Bx_h, nn, "Bx")) ||
             (r = h2d(By, By_h, nn, "By")) || (r = h2d(D, D_h, n2, "Dmat")) || (r = h2d(Dstrong, Ds_h, n2, "Dstrong")) ||
             (r = h2d(Dhat, Dh_h, n2, "Dhat")) || (r = h2d(Jinv, J_h, nn, "J")) || (r = h2d(q, q_h, nd, "q")) ||
-            (r = h2d(EleSizes, Es_h, (size_t)K, "ElementSizes")) || (r = h2d(Vinv, Vinv_h, n2, "VdmInv")) ||
+            (r = h2d(EleSizes, Es_h, (size_t)K, "ElementSizes")) || (r = h2d(Vinv, Vinv_h_, n2, "VdmInv")) ||
             (r = h2d(EdgeData, ED_h, (size_t)F * 8, "EdgeData")) || (r = h2d(ftab, ft.data(), (size_t)F, "faces")) ||
             (r = h2d(side, sd.data(), (size_t)K * 4, "sides")))
             return r;
@@ -253,6 +314,7 @@ class Engine {
         if (!PP_ && GLw_h && (r = h2d(GLw, GLw_h, (size_t)ngl, "GLw"))) return r;
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "copyDeviceVariables");
+        Vinv_h.assign(Vinv_h_, Vinv_h_ + n2);
         copied = true;
         return 0;
     }
@@ -291,6 +353,7 @@ class Engine {
     template <int NGL>
     int launch_face(bool av_grad) {
         FaceArgs a{F, ftab, q, nx, ny, scal, bL, bR, SP, SGX, SGY, elem_inst, st, phys()};
+        a.act = (AV && indicator) ? act : nullptr;
         const long n = (long)F * NGL;
         const int blocks = (int)((n + 255) / 256);
         if (av_grad) {
@@ -355,10 +418,27 @@ class Engine {
         using S = ElemShape<NGL>;
         const int eb = (K + S::NE - 1) / S::NE;
         const int lam_in_elem = (last && !PP) ? 1 : 0;
-        launch_face<NGL>(AV != 0);
-        if (!AV) {
+        if (AV && indicator) {
+            // active set: indicator (stages > 0; stage 0's runs before the
+            // step's dt), plain element kernel (flagged elements only write
+            // Qt and are listed), then gradient, viscous face flux and
+            // viscous update over the list
+            if (shock_stage) launch_indicator<NGL>(0);
+            launch_face<NGL>(true);
+            ElemArgs ea = elem_args(mode, A, Bc, C, lam_in_elem, 0);
+            ea.act = act; ea.alist = alist; ea.acount = act + K;
+            launch_elem_plain<NGL>(ea);
+            k_grad_list<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
+            const long n = (long)F * NGL;
+            k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
+                                                                         elem_inst, st, geomFace, act);
+            k_element_av2<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
+            launches += 3;
+        } else if (!AV) {
+            launch_face<NGL>(false);
             launch_elem_plain<NGL>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
         } else {
+            launch_face<NGL>(true);
             k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0, shock_stage ? 1 : 0));
             const long n = (long)F * NGL;
             k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
@@ -387,8 +467,106 @@ class Engine {
     }
 
     template <int NGL>
+    void launch_indicator(int stage0) {
+        cudaMemsetAsync(act, 0, (size_t)(K + 1) * sizeof(int), stream);
+        IndArgs ia;
+        ia.K = K; ia.q = q; ia.B = B; ia.Vinv = Vinv; ia.VP = VP; ia.act = act; ia.side = side; ia.ftab = ftab;
+        ia.elem_inst = elem_inst; ia.st = st; ia.c = phys(); ia.stage0 = stage0;
+        ia.P = mlpP; ia.Pb = mlpPb; ia.L = mlp_layout(NGL); ia.margin = ind_margin;
+        ia.emin = ind_emin; ia.emax = ind_emax; ia.stats = ind_stats;
+        const int blocks = (K + 16 * IND_WARPS - 1) / (16 * IND_WARPS);
+        if (indicator == 2)
+            k_indicator<NGL, true><<<blocks, IND_WARPS * 32, IndSmem<NGL>::bytes(true), stream>>>(ia);
+        else
+            k_indicator<NGL, false><<<blocks, IND_WARPS * 32, IndSmem<NGL>::bytes(false), stream>>>(ia);
+        ++launches;
+    }
+
+    template <int NGL>
+    int setup_indicator() {
+        cudaError_t e = cudaFuncSetAttribute(k_indicator<NGL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             IndSmem<NGL>::bytes(true));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_indicator<NGL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     IndSmem<NGL>::bytes(false));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (indicator)");
+        using S = ElemShape<NGL>;
+        int a2 = 0, gr = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a2, k_element_av2<NGL>, S::THREADS, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&gr, k_grad_list<NGL>, S::THREADS, 0);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return cuda_fail(e, "occupancy (list kernels)");
+        list_grid = std::max(1, std::min(std::max(1, std::min(a2, gr)) * sms, (K + S::NE - 1) / S::NE));
+        return 0;
+    }
+
+    // Selects the indicator (0, 1, 2; see `indicator`); P (mode 2) is the
+    // network's FP32 parameter block of mlp_layout(ngl).total floats.
+    int set_indicator(int mode, const float* P_h, int nP, float margin) {
+        if (!inited || !built) return fail(ESDG_E_ARG, "set_indicator after buildDeviceKernels");
+        if (mode < 0 || mode > 2) return fail(ESDG_E_ARG, "indicator mode must be 0, 1 or 2");
+        if (mode > 0 && !AV) return fail(ESDG_E_ARG, "the indicator needs ArtificialViscosity=1");
+        if (mode == 2) {
+            if (ngl < 3 || ngl > 6) return fail(ESDG_E_UNSUPPORTED, "the learned indicator supports N = 2..5");
+            if (!P_h || nP != mlp_layout(ngl).total)
+                return fail(ESDG_E_ARG, "learned indicator: parameter block of " +
+                                            std::to_string(mlp_layout(ngl).total) + " floats expected");
+            if (!(margin >= 0.0f)) return fail(ESDG_E_ARG, "learned indicator: margin must be >= 0");
+        }
+        int r = 0;
+        if (mode > 0 && !act) {
+            if ((r = alloc(&act, (size_t)K + 1)) || (r = alloc(&alist, (size_t)K)) || (r = alloc(&ind_stats, 4)))
+                return r;
+            switch (ngl) {
+                case 2: r = setup_indicator<2>(); break;
+                case 3: r = setup_indicator<3>(); break;
+                case 4: r = setup_indicator<4>(); break;
+                case 5: r = setup_indicator<5>(); break;
+                case 6: r = setup_indicator<6>(); break;
+                case 7: r = setup_indicator<7>(); break;
+                case 8: r = setup_indicator<8>(); break;
+            }
+            if (r) return r;
+        }
+        if (mode == 2) {
+            const int n = mlp_layout(ngl).total;
+            if (!mlpP && ((r = alloc(&mlpP, (size_t)n)) || (r = alloc(&mlpPb, (size_t)n)))) return r;
+            cudaError_t e = cudaMemcpyAsync(mlpP, P_h, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "indicator weights");
+            k_mlp_cast<<<(n + 255) / 256, 256, 0, stream>>>(n, mlpP, mlpPb);
+            // bounds of the sensor's modal energy n1 = |V m V^T|^2 over the
+            // nodal energy |m|^2: squares of the extreme eigenvalues of V^T V
+            double lo = 0, hi = 0;
+            gram_extremes(Vinv_h, ngl, &lo, &hi);
+            ind_emin = lo * lo * (1.0 - 1e-9);
+            ind_emax = hi * hi * (1.0 + 1e-9);
+            ind_margin = margin;
+            e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return cuda_fail(e, "indicator set-up");
+        }
+        indicator = mode;
+        if (graph) return capture_step_graph();
+        return 0;
+    }
+
+    int indicator_stats(unsigned long long* out4, int reset) {
+        if (!ind_stats) {
+            for (int k = 0; k < 4; ++k) out4[k] = 0;
+            return 0;
+        }
+        cudaError_t e = cudaMemcpyAsync(out4, ind_stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess && reset) e = cudaMemsetAsync(ind_stats, 0, 4 * sizeof(unsigned long long), stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "indicator stats");
+        return 0;
+    }
+
+    template <int NGL>
     void launch_step() {
-        if (AV) launch_shock<NGL>();
+        if (AV) {
+            if (indicator) launch_indicator<NGL>(1);
+            else launch_shock<NGL>();
+        }
         k_step_begin<<<(I + 127) / 128, 128, 0, stream>>>(I, st, ngl, AV);
         ++launches;
         if (rkSSP) {
@@ -580,6 +758,7 @@ class Engine {
         int r = check_ready();
         if (r) return r;
         if (gStages <= 0) return fail(ESDG_E_ARG, "profile_steps needs a previous esdg_dg_timeloop call");
+        if (AV && indicator) return fail(ESDG_E_UNSUPPORTED, "profile_steps times the reference path (indicator 0)");
         for (auto& e : pev)
             if (!e && cudaEventCreate(&e) != cudaSuccess) return fail(ESDG_E_CUDA, "cudaEventCreate");
         if ((r = poll_state())) return r;
@@ -804,6 +983,26 @@ int esdg_compute_rhs(esdg_deviceclass* d, double* Qt_host, double* visc_host) {
     ESDG_GUARD(d);
     if (!Qt_host) return d->eng.fail(ESDG_E_ARG, "null Qt");
     return d->eng.rhs(Qt_host, visc_host);
+}
+
+int esdg_set_indicator(esdg_deviceclass* d, int mode, const float* params, int nparams, float margin) {
+    ESDG_GUARD(d);
+    return d->eng.set_indicator(mode, params, nparams, margin);
+}
+
+int esdg_indicator_stats(esdg_deviceclass* d, unsigned long long* counts4, int reset) {
+    ESDG_GUARD(d);
+    if (!counts4) return d->eng.fail(ESDG_E_ARG, "null counts");
+    return d->eng.indicator_stats(counts4, reset);
+}
+
+int esdg_state_pointers(esdg_deviceclass* d, const double** q, const double** b, const double** VdmInv) {
+    ESDG_GUARD(d);
+    if (!d->eng.built) return d->eng.fail(ESDG_E_ARG, "state_pointers before buildDeviceKernels");
+    if (q) *q = d->eng.q;
+    if (b) *b = d->eng.B;
+    if (VdmInv) *VdmInv = d->eng.Vinv;
+    return ESDG_OK;
 }
 
 int esdg_set_stream(esdg_deviceclass* d, void* cuda_stream) {
@@ -1149,3 +1348,4 @@ extern "C" int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES
 }
 
 #include "esdg_arena.cuh"
+#include "esdg_mlp_abi.cuh"

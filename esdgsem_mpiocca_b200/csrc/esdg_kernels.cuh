@@ -46,6 +46,9 @@ struct FaceArgs {
     const int* __restrict__ elem_inst;
     const DevState* __restrict__ st;
     PhysConst c;
+    // active set (null: every face): gradient fluxes only where an adjacent
+    // element is flagged
+    const int* __restrict__ act = nullptr;
 };
 
 struct ElemArgs {
@@ -81,6 +84,12 @@ struct ElemArgs {
     int lam;         // 1: element wave speed max into st[inst].lam_key after the update
     int shock;       // AV: recompute the shock sensor into VP
     PhysConst c;
+    // Active set (null: none).  Plain element kernels write Qt instead of
+    // updating flagged elements and append them to alist (count in
+    // *acount); k_element_av2 and k_grad_list then run over alist only.
+    const int* __restrict__ act = nullptr;
+    int* alist = nullptr;
+    int* acount = nullptr;
 };
 
 __device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return elem_inst ? elem_inst[e] : 0; }
@@ -128,7 +137,7 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
     sp[0] = s * a.c.geomFace * N0;
     sp[NGL] = s * a.c.geomFace * N1;
     sp[2 * NGL] = s * a.c.geomFace * N2f;
-    if (AV) {
+    if (AV && (!a.act || a.act[eL] || (eR >= 0 && a.act[eR]))) {
         // okl/BR1_Gradient/calcNumFluxesGradient.okl:16-135 (the right trace
         // is taken in the right element's own order, as there).
         const double tol = a.c.PosPresTOL;
@@ -153,7 +162,7 @@ __global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict
                                                    const double* __restrict__ GX, const double* __restrict__ GY,
                                                    const double* __restrict__ VP, double* __restrict__ SPV,
                                                    const int* __restrict__ elem_inst, const DevState* __restrict__ st,
-                                                   double geomFace) {
+                                                   double geomFace, const int* __restrict__ act = nullptr) {
     const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long)F * NGL) return;
     constexpr int N2 = NGL * NGL;
@@ -163,7 +172,16 @@ __global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict
     if (st[inst_of(elem_inst, eL)].done) return;
     const long ex = (long)f * NGL + i;
     double N0 = 0.0, N1 = 0.0;
-    if (eR >= 0) {
+    // Active set: only faces of flagged elements are read.  A face with a
+    // non-flagged side has zero viscosity on both sides (a flagged
+    // neighbour would have flagged it), so its flux is zero.
+    bool need = true;
+    if (act) {
+        const bool aL = act[eL] != 0, aR = eR >= 0 && act[eR] != 0;
+        if (!aL && !aR) return;
+        need = aL && aR;
+    }
+    if (eR >= 0 && need) {
         const int inc = same ? i : NGL - 1 - i;
         const long oL = (long)eL * 2 * N2 + trace_offset(sL, i, NGL);
         const long oR = (long)eR * 2 * N2 + trace_offset(sR, inc, NGL);
@@ -252,6 +270,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
     double h = 0, hu = 0, hv = 0, J = 0, bx = 0, by = 0, o0 = 0, o1 = 0, o2 = 0, dt = 0;
     double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
     int ms[2] = {0, 0};
+    const bool to_list = active && a.act && a.act[e] != 0;
     if (active) {
         h = a.q[qid]; hu = a.q[qid + N2]; hv = a.q[qid + 2 * N2];
         sh[s] = h; shu[s] = hu; shv[s] = hv;
@@ -318,8 +337,9 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
                 r2 += -m * J * f[pass][2] + J * db;
             }
         }
-        if (a.mode == 2) {
+        if (a.mode == 2 || to_list) {
             a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
+            if (to_list && nd == 0) a.alist[atomicAdd(a.acount, 1)] = e;
         } else {
             double q0, q1, q2;
             if (a.mode == 0) {
@@ -339,7 +359,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
             if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
         }
     }
-    if (a.lam) warp_lambda<ElemShape<NGL>::THREADS>(lam, active, ins, a.st);
+    if (a.lam) warp_lambda<ElemShape<NGL>::THREADS>(lam, active && !to_list, ins, a.st);
 }
 
 // Modal energy sensor of one element (okl/ShockCapturing/ShockCapturing.okl:17-234),
@@ -526,21 +546,17 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av1(ElemArg
     }
 }
 
-// Viscous volume term + viscous lift added to Qt, then the RK update.
+// Viscous volume term + viscous lift added to Qt, then the RK update, for
+// the block's NE elements e0 + el (inb: element exists).
 // okl/ViscoseParts/VolumeKernelViscose.okl:17-150, SurfaceKernelVisc.okl:17-144.
 template <int NGL>
-__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av2(ElemArgs a) {
-    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
-    __shared__ double sDs[N2];
-    __shared__ double sF2[NE * N2], sF3[NE * N2], sG2[NE * N2], sG3[NE * N2];
+__device__ __forceinline__ void av2_tile(const ElemArgs& a, int e, bool inb, double* sDs, double* sF2, double* sF3,
+                                         double* sG2, double* sG3) {
+    constexpr int N2 = NGL * NGL;
     const int tid = threadIdx.x;
     const int el = tid / N2, nd = tid % N2;
-    const int e0 = blockIdx.x * NE;
-    const int e = e0 + el;
-    const bool inb = e < a.K;
     const int ins = inb ? inst_of(a.elem_inst, e) : 0;
     const bool active = inb && !a.st[ins].done;
-    if (tid < N2) sDs[tid] = a.Dstrong[tid];
     const long xid = (long)e * N2 + nd, qid = (long)e * 3 * N2 + nd, gid = (long)e * 2 * N2 + nd;
     const int s = el * N2 + nd;
     if (active) {
@@ -613,6 +629,107 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av2(ElemArg
         }
     }
     if (a.lam) warp_lambda<ElemShape<NGL>::THREADS>(lam, active, ins, a.st);
+}
+
+// Every element (alist null), or the elements of alist[0 .. *acount) with
+// a grid-stride loop over tiles of NE list entries.
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av2(ElemArgs a) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sDs[N2];
+    __shared__ double sF2[NE * N2], sF3[NE * N2], sG2[NE * N2], sG3[NE * N2];
+    const int tid = threadIdx.x;
+    const int el = tid / N2;
+    if (tid < N2) sDs[tid] = a.Dstrong[tid];
+    if (!a.alist) {
+        const int e = blockIdx.x * NE + el;
+        av2_tile<NGL>(a, e, e < a.K, sDs, sF2, sF3, sG2, sG3);
+        return;
+    }
+    const int count = *a.acount;
+    for (int t = blockIdx.x; t * NE < count; t += gridDim.x) {
+        const int idx = t * NE + el;
+        const bool inb = idx < count;
+        av2_tile<NGL>(a, inb ? a.alist[idx] : 0, inb, sDs, sF2, sF3, sG2, sG3);
+        __syncthreads();  // shared tiles are rewritten by the next iteration
+    }
+}
+
+// BR1 gradient (lifted, h-scaled) of the elements of alist[0 .. *acount):
+// the gradient part of k_element_av1, in the same arithmetic order.
+// okl/BR1_Gradient/calcGradient.okl:18-156, SurfaceKernelGradient.okl:16-150,
+// scaleGradient.okl:17-60.
+template <int NGL>
+__global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_grad_list(ElemArgs a) {
+    constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
+    __shared__ double sDh[N2];
+    __shared__ double su[NE * N2], sv[NE * N2];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int xi = nd % NGL, eta = nd / NGL;
+    if (tid < N2) sDh[tid] = a.Dhat[tid];
+    const int count = *a.acount;
+    for (int t = blockIdx.x; t * NE < count; t += gridDim.x) {
+        const int idx = t * NE + el;
+        const bool inb = idx < count;
+        const int e = inb ? a.alist[idx] : 0;
+        const long xid = (long)e * N2 + nd, qid = (long)e * 3 * N2 + nd;
+        const int s = el * N2 + nd;
+        double h = 0;
+        if (inb) {
+            h = a.q[qid];
+            const double hu = a.q[qid + N2], hv = a.q[qid + 2 * N2];
+            const double iv = (h > a.c.PosPresTOL) ? 1.0 / h : 0.0;
+            su[s] = hu * iv; sv[s] = hv * iv;
+        }
+        __syncthreads();
+        if (inb) {
+            const int rb = el * N2 + eta * NGL, cb = el * N2 + xi;
+            const double J = a.Jinv[xid];
+            const double ye = a.Yeta[xid], yx = a.Yxi[xid], xe = a.Xeta[xid], xx = a.Xxi[xid];
+            double gx0, gx1, gy0, gy1;
+            {
+                double uxi = 0, ueta = 0, vxi = 0, veta = 0;
+#pragma unroll
+                for (int l = 0; l < NGL; ++l) {
+                    uxi += sDh[xi * NGL + l] * su[rb + l];
+                    ueta += sDh[eta * NGL + l] * su[cb + l * NGL];
+                    vxi += sDh[xi * NGL + l] * sv[rb + l];
+                    veta += sDh[eta * NGL + l] * sv[cb + l * NGL];
+                }
+                const double ux = ye * uxi - yx * ueta, vx = ye * vxi - yx * veta;
+                const double uy = -xe * uxi + xx * ueta, vy = -xe * vxi + xx * veta;
+                gx0 = J * ux; gx1 = J * vx; gy0 = J * uy; gy1 = J * vy;
+            }
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                int side = -1, j = 0;
+                if (pass == 0) {
+                    if (eta == 0) { side = 0; j = xi; }
+                    else if (eta == NGL - 1) { side = 2; j = xi; }
+                } else {
+                    if (xi == NGL - 1) { side = 1; j = eta; }
+                    else if (xi == 0) { side = 3; j = eta; }
+                }
+                if (side >= 0) {
+                    const int4 sd = a.side[(long)e * 4 + side];
+                    const int inc = sd.z ? j : NGL - 1 - j;
+                    const int ms = sd.y;
+                    const double* ux = a.SGX + (long)sd.x * 2 * NGL + inc;
+                    const double* uy = a.SGY + (long)sd.x * 2 * NGL + inc;
+                    if (pass == 0) gx0 += ms * ux[0] * J;
+                    else gx0 += ms * J * ux[0];
+                    gx1 += ms * J * ux[NGL];
+                    gy0 += ms * J * uy[0];
+                    gy1 += ms * J * uy[NGL];
+                }
+            }
+            const long gid = (long)e * 2 * N2 + nd;
+            a.GX[gid] = h * gx0; a.GX[gid + N2] = h * gx1;
+            a.GY[gid] = h * gy0; a.GY[gid + N2] = h * gy1;
+        }
+        __syncthreads();
+    }
 }
 
 // Positivity limiter (okl/Positivity/PosPres.okl:17-223), optionally with the

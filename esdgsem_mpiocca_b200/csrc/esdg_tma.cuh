@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, ESDG_TMA_MIN_BLOCKS) k
         const bool inb = e < a.K;
         const int ins = inb ? inst_of(a.elem_inst, e) : 0;
         const bool active = inb && !a.st[ins].done;
+        const bool to_list = active && a.act && a.act[e] != 0;
         // face fluxes of this node's sides (global, mostly L2) before the wait
         double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
         int ms[2] = {0, 0};
@@ -277,8 +278,9 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, ESDG_TMA_MIN_BLOCKS) k
                 }
             }
             const long qid = (long)e * 3 * N2 + nd;
-            if (a.mode == 2) {
+            if (a.mode == 2 || to_list) {
                 a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
+                if (to_list && nd == 0) a.alist[atomicAdd(a.acount, 1)] = e;
             } else {
                 const double o0 = s2[qs], o1 = s2[qs + N2], o2 = s2[qs + 2 * N2];
                 double q0, q1, q2;
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, ESDG_TMA_MIN_BLOCKS) k
                 if (a.lam) lam = node_lambda(a.c, q0, q1, q2);
             }
         }
-        if (a.lam) warp_lambda<S::THREADS>(lam, active, ins, a.st);
+        if (a.lam) warp_lambda<S::THREADS>(lam, active && !to_list, ins, a.st);
         __syncthreads();  // stage buffer and si free again
         if (tid == 0) {
             const int tn = t + ST * gridDim.x;

@@ -29,6 +29,13 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+def _indicator_params(net):
+    if net is None:
+        raise ValueError("the learned indicator needs a network")
+    P = np.ascontiguousarray(net.P, dtype=np.float32)
+    return P.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), P.size, float(net.margin)
+
+
 class DeviceClass:
     """One engine handle (one GPU, one mesh)."""
 
@@ -127,6 +134,28 @@ class DeviceClass:
     def kernel_launches(self) -> int:
         return int(self._L.esdg_kernel_launches(self.h))
 
+    def set_indicator(self, mode: int, net=None):
+        """Indicator of the artificial-viscosity path: 0 the modal sensor and
+        the viscous terms everywhere (the reference's path), 1 the modal
+        sensor with the active set, 2 the learned indicator (`net`, an
+        indicator.IndicatorNet) with the active set."""
+        P, n, margin = _indicator_params(net) if mode == 2 else (None, 0, 0.0)
+        self._ok(self._L.esdg_set_indicator(self.h, mode, P, n, margin))
+
+    def indicator_stats(self, reset: bool = False):
+        """Counts since the last reset: elements set to zero by the network,
+        set to eps0 by the network, decided by the modal sensor, and with
+        nonzero viscosity."""
+        out = (ctypes.c_ulonglong * 4)()
+        self._ok(self._L.esdg_indicator_stats(self.h, out, int(reset)))
+        return dict(zip(("net_zero", "net_full", "modal", "viscous"), [int(v) for v in out]))
+
+    def state_pointers(self):
+        """Device addresses (q, b, VdmInv) of the engine's own buffers."""
+        q, b, v = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        self._ok(self._L.esdg_state_pointers(self.h, ctypes.byref(q), ctypes.byref(b), ctypes.byref(v)))
+        return q.value, b.value, v.value
+
     def close(self):
         if self.h is not None and self.h.value:
             self._L.esdg_deviceclass_destroy(self.h)
@@ -142,7 +171,7 @@ class DeviceClass:
 class Solver:
     """main.cpp:925-1051 for one Problem: init, copy, build, time loop."""
 
-    def __init__(self, prob: Problem, device_id: int = -1, q0=None):
+    def __init__(self, prob: Problem, device_id: int = -1, q0=None, indicator: int = 0, net=None):
         self.prob = prob
         p, m, bs = prob.params, prob.mesh, prob.basis
         self.dc = DeviceClass(0, device_id)
@@ -157,6 +186,8 @@ class Solver:
                                     m.MasterSlave, m.Orientation, m.ElemToEdge, m.EdgeData, m.EdgeReversed)
         self.dc.buildDeviceKernels(99, 99, p.Testcase, p.FluxDifferencing, p.NumFlux, p.rkSSP, p.ArtificialViscosity,
                                    p.PositivityPreserving, p.DiscBottom)
+        if indicator:
+            self.dc.set_indicator(indicator, net)
 
     def run(self, T=None, max_steps=None):
         p, prob = self.prob.params, self.prob

@@ -87,6 +87,19 @@ class Ensemble:
     def kernel_launches(self) -> int:
         return int(self._L.esdg_ensemble_kernel_launches(self.h))
 
+    def set_indicator(self, mode: int, net=None):
+        """0: modal sensor and viscous terms everywhere (the reference's
+        path); 1: modal sensor with the active set; 2: the learned indicator
+        (indicator.IndicatorNet) with the active set."""
+        from .deviceclass import _indicator_params
+        P, n, margin = _indicator_params(net) if mode == 2 else (None, 0, 0.0)
+        self._ok(self._L.esdg_ensemble_set_indicator(self.h, mode, P, n, margin))
+
+    def indicator_stats(self, reset: bool = False):
+        out = (ctypes.c_ulonglong * 4)()
+        self._ok(self._L.esdg_ensemble_indicator_stats(self.h, out, int(reset)))
+        return dict(zip(("net_zero", "net_full", "modal", "viscous"), [int(v) for v in out]))
+
     def set_stream(self, stream_ptr):
         self._ok(self._L.esdg_ensemble_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
 

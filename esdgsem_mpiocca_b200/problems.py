@@ -88,6 +88,39 @@ def dam_break(N=4, nel=256, seed=0, steps=2000, NumFlux=0, CFL=0.4, AV=1, eps0=N
                         {"name": "dam_break", "nel": nel, "seed": seed, "radius": r0, "centre": (cx, cy)})
 
 
+def bore(N=4, nel=256, seed=0, steps=2000, NumFlux=0, CFL=0.4, AV=1, eps0=None, sigma_min=None, sigma_max=None,
+         rotate_seed=0) -> Problem:
+    """A straight bore on the curved unit square (walls, b = 0): depth h_L
+    behind the front s = x cos(a) + y sin(a) = s0, h_R = 1 ahead at rest, and
+    the flow behind moving with the Rankine-Hugoniot velocity of a bore
+    running into still water, u_L = S (1 - h_R / h_L) with
+    S = sqrt(g h_L (h_L + h_R) / (2 h_R)); h_L ~ U[1.1, 1.8], a ~ U[0, 2 pi),
+    s0 chosen so that the front crosses the middle of the domain."""
+    rng = np.random.default_rng(50_000 + seed)
+    g = 9.81
+    hL, hR = rng.uniform(1.1, 1.8), 1.0
+    a = rng.uniform(0.0, 2.0 * np.pi)
+    S = np.sqrt(g * hL * (hL + hR) / (2.0 * hR))
+    uL = S * (1.0 - hR / hL)
+    p = Params(N=N, CFL=CFL, DFL=0.1, T=1.0e9, g_const=g, NumFlux=NumFlux, ES=1, rkOrder=4, rkSSP=0,
+               ArtificialViscosity=AV, MaxSteps=steps,
+               epsilon_0=0.01 if eps0 is None else eps0,
+               sigma_min=-6.0 if sigma_min is None else sigma_min,
+               sigma_max=-2.0 if sigma_max is None else sigma_max)
+    m = mesh_mapped(N, 0.0, 1.0, 0.0, 1.0, nel, nel, amp=0.03, rotate_seed=rotate_seed)
+    x, y = m.x, m.y
+    s = (x - 0.5) * np.cos(a) + (y - 0.5) * np.sin(a)
+    s0 = rng.uniform(-0.3, -0.1)
+    behind = s < s0
+    h = np.where(behind, hL, hR)
+    hu = np.where(behind, hL * uL * np.cos(a), 0.0)
+    hv = np.where(behind, hL * uL * np.sin(a), 0.0)
+    b = np.zeros_like(x)
+    n2 = (N + 1) ** 2
+    return make_problem(p, m, b, _state(h, hu, hv, K=m.K, n2=n2),
+                        {"name": "bore", "nel": nel, "seed": seed, "hL": hL, "angle": a})
+
+
 TSUNAMI_SIZES = (64, 96, 128, 192, 256)
 
 

@@ -152,6 +152,133 @@ int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES, double g_
                              const int* ElemEdgeMasterSlave, const int* ElemEdgeOrientation, double* Qt,
                              void* stream);
 
+/* Device addresses of the solution q [K][3][(N+1)^2], the bathymetry b
+ * [K][(N+1)^2] and VdmInv [(N+1)^2] owned by the engine (no counterpart in
+ * the reference), for device-side consumers such as the indicator's
+ * training-data extraction.  Valid until esdg_free_occa_vars. */
+int esdg_state_pointers(esdg_deviceclass* d, const double** q, const double** b, const double** VdmInv);
+
+/* Troubled-cell indicator of the artificial-viscosity path (no counterpart
+ * in the reference; call after esdg_build_device_kernels with
+ * ArtificialViscosity=1):
+ *   mode 0  the reference's path: the modal sensor
+ *           (okl/ShockCapturing/ShockCapturing.okl:17-234) and the viscous
+ *           terms on every element (the default);
+ *   mode 1  the modal sensor with the active set: the BR1 gradient and the
+ *           viscous terms run only on elements with viscosity > 0 and their
+ *           face neighbours (everywhere else they are exactly zero), so the
+ *           solution is the same as with mode 0;
+ *   mode 2  the learned indicator with the active set: the network whose
+ *           FP32 parameter block (esdg_mlp_layout(N+1).total floats) is
+ *           `params` sets viscosity 0 where it predicts
+ *           sigma < sigma_min - margin and eps0 where it predicts
+ *           sigma > sigma_max + margin; the modal sensor decides every other
+ *           element (the ramp band, positivity check failures, modal energy
+ *           near ZeroTOL).  N in 2..5.
+ * params/nparams/margin are ignored for modes 0 and 1. */
+int esdg_set_indicator(esdg_deviceclass* d, int mode, const float* params, int nparams, float margin);
+
+/* Decision counts accumulated over indicator launches: [0] elements the
+ * network set to zero, [1] set to eps0, [2] decided by the modal sensor,
+ * [3] elements with nonzero viscosity; reset != 0 zeroes them. */
+int esdg_indicator_stats(esdg_deviceclass* d, unsigned long long* counts4, int reset);
+
+/* ------------------------------------------------------------------------
+ * Batched ensemble (no counterpart in the reference, which runs one mesh
+ * per process): independent instances of one polynomial degree N advanced
+ * together, each kernel launch covering every instance, each instance with
+ * its own time, time step, end time and step cap.  Instances are added and
+ * removed between advances; the captured step graph stays valid.
+ * ---------------------------------------------------------------------- */
+
+typedef struct esdg_ensemble esdg_ensemble;
+
+/* Capacity for max_instances instances holding up to K_capacity elements
+ * and F_capacity faces in total; the solver switches are those of
+ * initDeviceVariables/buildDeviceKernels, shared by every instance. */
+int esdg_ensemble_create(int device_id, int N, int max_instances, int K_capacity, int F_capacity, int NumFlux, int ES,
+                         double g_const, double PosPresTOL, int ArtificialViscosity, double epsilon_0,
+                         double sigma_max, double sigma_min, int PositivityPreserving, int rkOrder, int rkSSP,
+                         esdg_ensemble** out);
+
+/* Adds one instance (host arrays as for esdg_copy_device_variables, its own
+ * numbering; J is 1/J), running until t >= T or max_steps steps (0: no cap);
+ * *id receives its slot.  ESDG_E_NOMEM when no contiguous capacity is free. */
+int esdg_ensemble_add(esdg_ensemble* en, int Nelem, int Nfaces, const double* normalsX, const double* normalsY,
+                      const double* Scal, const double* y_xi, const double* y_eta, const double* x_xi,
+                      const double* x_eta, const double* b, const double* Bx, const double* By, const double* J,
+                      const double* q, const double* ElementSizes, const int* ElemEdgeMasterSlave,
+                      const int* ElemEdgeOrientation, const int* ElemToEdge, const int* EdgeData, double T,
+                      int max_steps, double minEleSize, double CFL, double DFL, int* id);
+
+/* Releases an instance's slot and capacity (its results are gone). */
+int esdg_ensemble_remove(esdg_ensemble* en, int id);
+
+/* Replays the step graph nsteps times (finished instances are skipped on
+ * the device) and refreshes the host copy of every instance's status. */
+int esdg_ensemble_advance(esdg_ensemble* en, int nsteps);
+
+/* Status from the last advance: time, steps taken, done flag, status
+ * (0 ok, 1 non-finite wave speed). */
+int esdg_ensemble_status(esdg_ensemble* en, int id, double* t, int* steps, int* done, int* status);
+
+/* Copies an instance's q [Nelem*3*(N+1)^2] to the host. */
+int esdg_ensemble_copy_q(esdg_ensemble* en, int id, double* q);
+
+/* Largest free contiguous element and face ranges and the free slot count. */
+int esdg_ensemble_free_capacity(const esdg_ensemble* en, int* K_largest, int* F_largest, int* free_slots);
+
+long long esdg_ensemble_bytes(const esdg_ensemble* en);
+long long esdg_ensemble_kernel_launches(const esdg_ensemble* en);
+
+/* Runs on the caller's stream (NULL: the ensemble's own); re-captures the
+ * step graph. */
+int esdg_ensemble_set_stream(esdg_ensemble* en, void* cuda_stream);
+/* esdg_set_indicator / esdg_indicator_stats for every instance of the
+ * ensemble (re-captures the step graph). */
+int esdg_ensemble_set_indicator(esdg_ensemble* en, int mode, const float* params, int nparams, float margin);
+int esdg_ensemble_indicator_stats(esdg_ensemble* en, unsigned long long* counts4, int reset);
+const char* esdg_ensemble_last_error(const esdg_ensemble* en);
+int esdg_ensemble_destroy(esdg_ensemble* en);
+
+/* ------------------------------------------------------------------------
+ * Learned troubled-cell indicator: training kernels (no counterpart in the
+ * reference).  A 3-layer MLP (F -> 32 -> 32 -> 1, ReLU) predicting the modal
+ * shock sensor's sigma = log10(energy ratio) of an element
+ * (okl/ShockCapturing/ShockCapturing.okl:131-204) from its features; BF16
+ * weights and activations on the tensor cores, FP32 accumulation, FP32
+ * master weights.  ngl = N+1 in 3..6.  Every pointer is a device pointer;
+ * calls are asynchronous on `stream` (NULL: legacy default stream).
+ * Failures are described by esdg_last_error(NULL).
+ * ---------------------------------------------------------------------- */
+
+/* Parameter block layout in floats: kp (row length of X and W1), offsets
+ * of W1[32][kp], b1[32], W2[32][32], b2[32], w3[32], b3, and the total. */
+int esdg_mlp_layout(int ngl, int* out8);
+
+/* Feature rows X [K][kp] (bf16) of the elements of q/b; when tgt is given,
+ * the training target clamp(sigma, -12, 0) - s_eta [K] (float); when seta
+ * is given, s_eta [K] (the log energy fraction of h + b's deviation). */
+int esdg_mlp_features(int ngl, int K, const double* q, const double* b, const double* VdmInv, double ZeroTOL, void* X,
+                      float* tgt, float* seta, void* stream);
+
+/* Pb (bf16) = P (float) over the whole block. */
+int esdg_mlp_cast(int ngl, const float* P, void* Pb, void* stream);
+
+/* y [M] = network output for the rows of X; `blocks` CTAs of 4 warps. */
+int esdg_mlp_forward(int ngl, int M, const void* X, const float* P, const void* Pb, float* y, int blocks,
+                     void* stream);
+
+/* Per-warp partial gradients of (1/M) sum (y - t)^2: partial [blocks*4][total]
+ * (slot b3+1 of each row: that warp's sum of squared errors). */
+int esdg_mlp_backward(int ngl, int M, const void* X, const float* tgt, const float* P, const void* Pb,
+                      float* partial, int blocks, void* stream);
+
+/* G = sum of the `rows` partial rows (fixed order), then one Adam step
+ * (step >= 1) on P, m, v, refreshing Pb. */
+int esdg_mlp_adam(int ngl, int rows, const float* partial, float* G, float* P, void* Pb, float* m, float* v,
+                  float lr, float beta1, float beta2, float eps, int step, void* stream);
+
 /* ------------------------------------------------------------------------
  * Host set-up (no GPU needed).
  * ---------------------------------------------------------------------- */
