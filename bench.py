@@ -167,6 +167,8 @@ def main():
                     help="curved_lake: the headline single-mesh workload; ensemble: 256 seeded tsunami "
                          "members batched vs one at a time")
     ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--alone-members", type=int, default=15,
+                    help="ensemble workload: members solved one at a time for the plain-path rate")
     args = ap.parse_args()
     if args.workload == "ensemble":
         return ensemble_bench(args)
@@ -307,77 +309,137 @@ def member_sizes(seeds):
     return out
 
 
+def _alone_sample(seeds, k):
+    """k members spread over the size classes (every class represented)."""
+    from esdgsem_mpiocca_b200.problems import TSUNAMI_SIZES
+    by = {n: [] for n in TSUNAMI_SIZES}
+    for sd, (K, _) in zip(seeds, member_sizes(seeds)):
+        by[int(round(K ** 0.5))].append(sd)
+    out = []
+    while len(out) < min(k, len(seeds)):
+        for n in TSUNAMI_SIZES:
+            if by[n] and len(out) < k:
+                out.append(by[n].pop(0))
+    return out
+
+
 def ensemble_bench(args):
-    """Config 4: 256 tsunami members (N=3, K in {64..256}^2, 500 steps each,
-    artificial viscosity with the modal sensor) advanced in one arena, vs the
-    same kind of members solved one at a time by the single-mesh engine."""
+    """The ensemble configuration: seeded tsunami members (N=3, K in
+    {64..256}^2 on 2000 km squares, artificial viscosity) advanced in one
+    arena with the learned indicator and the active set, against the plain
+    path -- the same members solved one at a time by the single-mesh engine
+    with the modal sensor and the viscous terms on every element.  Reports
+    both rates, their ratio, the batched rate of the other indicator modes
+    (attribution), and the largest relative L2 deviation of a batched
+    learned member from its plain one-at-a-time solution."""
     import torch
     from esdgsem_mpiocca_b200 import problems
     from esdgsem_mpiocca_b200.deviceclass import Solver
     from esdgsem_mpiocca_b200.ensemble import Ensemble
+    from esdgsem_mpiocca_b200.indicator import IndicatorNet
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     steps = args.steps if args.steps != 400 else 500
+    warm = max(args.warmup, 3)
+    total = warm + steps
     seeds = list(range(rank * args.members, (rank + 1) * args.members))
     sizes = member_sizes(seeds)
     Kc, Fc = sum(k for k, _ in sizes), sum(f for _, f in sizes)
-    p0 = problems.tsunami_member(seeds[0], steps=steps, sizes=(8,))  # parameters only
-    ens = Ensemble(3, len(seeds), Kc, Fc, NumFlux=p0.params.NumFlux, g_const=p0.params.g_const,
-                   PosPresTOL=p0.params.PosPresTOL, ArtificialViscosity=p0.params.ArtificialViscosity,
-                   epsilon_0=p0.params.epsilon_0, sigma_max=p0.params.sigma_max, sigma_min=p0.params.sigma_min)
+    p0 = problems.tsunami_member(seeds[0], steps=steps, sizes=(8,)).params  # parameters only
+    net = IndicatorNet.default(3)
+    sample = _alone_sample(seeds, args.alone_members)
+    attr_steps = min(steps, 50)
+    ens = Ensemble(3, len(seeds), Kc, Fc, NumFlux=p0.NumFlux, g_const=p0.g_const, PosPresTOL=p0.PosPresTOL,
+                   ArtificialViscosity=p0.ArtificialViscosity, epsilon_0=p0.epsilon_0,
+                   sigma_max=p0.sigma_max, sigma_min=p0.sigma_min, device_id=local)
+    ens.set_indicator(2, net)
     t0 = time.perf_counter()
-    dofs = 0
-    ids = []
+    dofs, ids, kept = 0, {}, {}
     for sd in seeds:
-        pr = problems.tsunami_member(sd, steps=steps)
-        ids.append(ens.add(pr, T=1e9, max_steps=steps))
+        pr = problems.tsunami_member(sd)
+        ids[sd] = ens.add(pr, T=1e9, max_steps=total + 2 * attr_steps)
         dofs += pr.dofs()
+        if sd in sample:
+            kept[sd] = pr
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.Stream()
     ens.set_stream(stream.cuda_stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    launches0 = ens.kernel_launches()
-    with Clocks(local) as ck:
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            ens.advance(steps)   # every member runs exactly `steps` steps
-            e1.record(stream)
+
+    def timed(nsteps):
+        ens.indicator_stats(reset=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    done = all(ens.status(i)["done"] or ens.status(i)["steps"] == steps for i in ids)
-    bad = [i for i in ids if ens.status(i)["status"] != 0]
-    batched = dofs * STAGES * steps / (ms / 1e3)
-    launches = ens.kernel_launches() - launches0
+        l0 = ens.kernel_launches()
+        with Clocks(local) as ck:
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                ens.advance(nsteps)
+                e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = [ens.status(i) for i in ids.values()]
+        return {"ms": ms, "rate": dofs * STAGES * nsteps / (ms / 1e3), "launches": ens.kernel_launches() - l0,
+                "stats": ens.indicator_stats(), "clocks": ck.result, "steps": [x["steps"] for x in st],
+                "errors": sum(1 for x in st if x["status"] != 0)}
+
+    # batched, learned indicator with the active set: W untimed steps, then
+    # the timed steps; the sampled members' states are kept for the
+    # deviation check
+    ens.advance(warm)
+    learned = timed(steps)
+    learned["all_done"] = all(x == total for x in learned["steps"])
+    qb = {sd: ens.q(ids[sd]) for sd in sample}
+    # attribution: the same arena continued with the other indicator modes
+    attrib = {}
+    for m in (0, 1):
+        ens.set_indicator(m)
+        attrib[m] = timed(attr_steps)
     ens.close()
-    # one at a time: members of every size, each alone on the GPU
-    alone_seeds = seeds[: min(len(seeds), 10)]
-    adofs, ams = 0, 0.0
-    for sd in alone_seeds:
-        pr = problems.tsunami_member(sd, steps=steps)
+    # one at a time, plain path (modal sensor, viscous terms everywhere)
+    adofs, ams, dev = 0, 0.0, 0.0
+    for sd in sample:
+        pr = kept[sd]
         s = Solver(pr, device_id=local)
         st = torch.cuda.Stream()
         s.dc.set_stream(st.cuda_stream)
+        s.run(T=1e9, max_steps=warm)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
         with torch.cuda.stream(st):
             a0.record(st)
-            s.run(T=1e9, max_steps=steps)
+            s.dc.advance(steps, 1e9)
             a1.record(st)
         torch.cuda.synchronize()
         ams += a0.elapsed_time(a1)
         adofs += pr.dofs()
+        qa = s.q().reshape(pr.K, 3, -1)
+        qm = qb[sd].reshape(pr.K, 3, -1)
+        for v in range(3):
+            dev = max(dev, float(np.linalg.norm(qm[:, v] - qa[:, v]) / max(np.linalg.norm(qa[:, v]), 1e-300)))
         s.close()
     alone = adofs * STAGES * steps / (ams / 1e3)
-    line = {"metric": METRIC, "value": batched * ws, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": 0,
-            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded tsunami members: shelf, seamounts, Okada uplift)",
+    stt = learned["stats"]
+    decided = stt["net_zero"] + stt["net_full"]
+    evals = decided + stt["modal"]
+    line = {"metric": METRIC, "value": learned["rate"] * ws, "unit": UNIT, "n_gpus": ws, "steps": steps,
+            "warmup": warm, "ms_per_step": learned["ms"] / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (indicator network: bf16 weights, fp32 accumulation)",
+            "data": "synthetic (seeded tsunami members: shelf, seamounts, Okada uplift)",
             "config": {"workload": f"ensemble of {len(seeds)} tsunami members, N=3, K in {{64..256}}^2 on 2000 km "
-                                   f"squares, {steps} LS-RK4 steps each, artificial viscosity (modal sensor)",
-                       "members": len(seeds), "nodes": dofs, "setup_s": setup_s, "all_done": bool(done),
-                       "members_with_error": len(bad)},
-            "one_at_a_time": {"value": alone, "unit": UNIT, "members": len(alone_seeds),
-                              "ratio_batched_over_alone": batched / alone},
-            "gpu_launches": int(launches), "clocks": ck.result}
+                                   f"squares, {steps} LS-RK4 steps each, artificial viscosity; batched arena with "
+                                   "the learned indicator and the active set",
+                       "members": len(seeds), "nodes": dofs, "setup_s": setup_s, "all_done": learned["all_done"],
+                       "members_with_error": learned["errors"],
+                       "l2": "state (~16 GB at 256 members) far larger than L2"},
+            "plain_one_at_a_time": {"value": alone, "unit": UNIT, "members": len(sample),
+                                    "note": "modal sensor and viscous terms on every element (reference path)"},
+            "ratio_batched_learned_over_plain": learned["rate"] / alone,
+            "max_rel_l2_deviation_vs_plain": dev,
+            "indicator": {"network_settled": decided / max(evals, 1), "modal_fallback": stt["modal"] / max(evals, 1),
+                          "viscous_share": stt["viscous"] / max(evals, 1), "margin": net.margin},
+            "attribution_batched": {"modal_full_path": attrib[0]["rate"], "modal_active_set": attrib[1]["rate"],
+                                    "learned_active_set": learned["rate"], "steps": attr_steps},
+            "gpu_launches": int(learned["launches"]), "clocks": learned["clocks"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

@@ -182,6 +182,7 @@ class Arena : public Engine {
         k_collect_bottom_impl<<<(F_ * ngl + 255) / 256, 256, 0, stream>>>(F_, ngl, EdgeData + fo * 8, B, bL + fo * ngl,
                                                                           bR + fo * ngl);
         ranged_lambda(re);
+        if (nbr) k_build_nbr<<<(K_ + 255) / 256, 256, 0, stream>>>(re.begin, K_, side, ftab, nbr);
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "arena add");
         inst[slot].live = true;

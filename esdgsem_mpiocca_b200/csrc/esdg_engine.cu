@@ -141,9 +141,11 @@ class Engine {
     double ind_emin = 0.0, ind_emax = 0.0;
     int* act = nullptr;                       // [K + 1]: flags, then the list length
     int* alist = nullptr;                     // [K] flagged elements of the stage
+    int4* nbr = nullptr;                      // [K] face neighbours
     unsigned long long* ind_stats = nullptr;  // [4] decision counts
     std::vector<double> Vinv_h;
     int list_grid = 0;                        // persistent grid of the list kernels
+    int ind_grid[2] = {1, 1};                 // persistent grids of the indicator (modal, learned)
 
     // step graph
     cudaGraphExec_t graph = nullptr;
@@ -184,7 +186,7 @@ class Engine {
         bytes = 0;
         if (st_host) { cudaFreeHost(st_host); st_host = nullptr; }
         q = gRK = Qt = Qtmp = nullptr;
-        mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr;
+        mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr; nbr = nullptr;
         indicator = 0;
         inited = copied = built = false;
     }
@@ -200,6 +202,7 @@ class Engine {
         c.sigmaMin = sigma_min;
         c.sigmaMax = sigma_max;
         c.ZeroTOL = std::pow(10.0, -5);
+        c.sensor_skip = std::isfinite(sigma_min) ? std::pow(10.0, sigma_min) * (1.0 - 1e-12) : 0.0;
         c.ES = ES;
         return c;
     }
@@ -470,33 +473,35 @@ class Engine {
     void launch_indicator(int stage0) {
         cudaMemsetAsync(act, 0, (size_t)(K + 1) * sizeof(int), stream);
         IndArgs ia;
-        ia.K = K; ia.q = q; ia.B = B; ia.Vinv = Vinv; ia.VP = VP; ia.act = act; ia.side = side; ia.ftab = ftab;
+        ia.K = K; ia.q = q; ia.B = B; ia.Vinv = Vinv; ia.VP = VP; ia.act = act; ia.nbr = nbr;
         ia.elem_inst = elem_inst; ia.st = st; ia.c = phys(); ia.stage0 = stage0;
         ia.P = mlpP; ia.Pb = mlpPb; ia.L = mlp_layout(NGL); ia.margin = ind_margin;
         ia.emin = ind_emin; ia.emax = ind_emax; ia.stats = ind_stats;
-        const int blocks = (K + 16 * IND_WARPS - 1) / (16 * IND_WARPS);
+        using S = IndShape<NGL>;
+        const int ntiles = (K + S::NE - 1) / S::NE;
         if (indicator == 2)
-            k_indicator<NGL, true><<<blocks, IND_WARPS * 32, IndSmem<NGL>::bytes(true), stream>>>(ia);
+            k_indicator<NGL, true><<<std::min(ntiles, ind_grid[1]), S::THREADS, 0, stream>>>(ia, ntiles);
         else
-            k_indicator<NGL, false><<<blocks, IND_WARPS * 32, IndSmem<NGL>::bytes(false), stream>>>(ia);
+            k_indicator<NGL, false><<<std::min(ntiles, ind_grid[0]), S::THREADS, 0, stream>>>(ia, ntiles);
         ++launches;
     }
 
     template <int NGL>
     int setup_indicator() {
-        cudaError_t e = cudaFuncSetAttribute(k_indicator<NGL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             IndSmem<NGL>::bytes(true));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_indicator<NGL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     IndSmem<NGL>::bytes(false));
-        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute (indicator)");
         using S = ElemShape<NGL>;
         int a2 = 0, gr = 0, sms = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a2, k_element_av2<NGL>, S::THREADS, 0);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a2, k_element_av2<NGL>, S::THREADS, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&gr, k_grad_list<NGL>, S::THREADS, 0);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy (list kernels)");
         list_grid = std::max(1, std::min(std::max(1, std::min(a2, gr)) * sms, (K + S::NE - 1) / S::NE));
+        int o0 = 0, o1 = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o0, k_indicator<NGL, false>, IndShape<NGL>::THREADS, 0);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_indicator<NGL, true>, IndShape<NGL>::THREADS, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "occupancy (indicator)");
+        ind_grid[0] = std::max(1, o0) * sms;
+        ind_grid[1] = std::max(1, o1) * sms;
         return 0;
     }
 
@@ -507,7 +512,7 @@ class Engine {
         if (mode < 0 || mode > 2) return fail(ESDG_E_ARG, "indicator mode must be 0, 1 or 2");
         if (mode > 0 && !AV) return fail(ESDG_E_ARG, "the indicator needs ArtificialViscosity=1");
         if (mode == 2) {
-            if (ngl < 3 || ngl > 6) return fail(ESDG_E_UNSUPPORTED, "the learned indicator supports N = 2..5");
+            if (ngl < 4 || ngl > 6) return fail(ESDG_E_UNSUPPORTED, "the learned indicator supports N = 3..5");
             if (!P_h || nP != mlp_layout(ngl).total)
                 return fail(ESDG_E_ARG, "learned indicator: parameter block of " +
                                             std::to_string(mlp_layout(ngl).total) + " floats expected");
@@ -515,8 +520,13 @@ class Engine {
         }
         int r = 0;
         if (mode > 0 && !act) {
-            if ((r = alloc(&act, (size_t)K + 1)) || (r = alloc(&alist, (size_t)K)) || (r = alloc(&ind_stats, 4)))
+            if ((r = alloc(&act, (size_t)K + 1)) || (r = alloc(&alist, (size_t)K)) || (r = alloc(&ind_stats, 4)) ||
+                (r = alloc(&nbr, (size_t)K)))
                 return r;
+            // the zero fills ran on the legacy stream
+            cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+            k_build_nbr<<<(K + 255) / 256, 256, 0, stream>>>(0, K, side, ftab, nbr);
             switch (ngl) {
                 case 2: r = setup_indicator<2>(); break;
                 case 3: r = setup_indicator<3>(); break;
@@ -530,7 +540,11 @@ class Engine {
         }
         if (mode == 2) {
             const int n = mlp_layout(ngl).total;
-            if (!mlpP && ((r = alloc(&mlpP, (size_t)n)) || (r = alloc(&mlpPb, (size_t)n)))) return r;
+            if (!mlpP) {
+                if ((r = alloc(&mlpP, (size_t)n)) || (r = alloc(&mlpPb, (size_t)n))) return r;
+                cudaError_t e = cudaDeviceSynchronize();
+                if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+            }
             cudaError_t e = cudaMemcpyAsync(mlpP, P_h, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, stream);
             if (e != cudaSuccess) return cuda_fail(e, "indicator weights");
             k_mlp_cast<<<(n + 255) / 256, 256, 0, stream>>>(n, mlpP, mlpPb);
@@ -1324,7 +1338,7 @@ extern "C" int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES
     PhysConst c;
     c.g = g_const; c.half_g = 0.5 * g_const; c.fourth_g = 0.25 * g_const;
     c.geomFace = 1.0 / (2.0 / (N * (N + 1.0)));
-    c.PosPresTOL = PosPresTOL; c.eps0 = 0; c.sigmaMin = 0; c.sigmaMax = 0; c.ZeroTOL = std::pow(10.0, -5); c.ES = ES;
+    c.PosPresTOL = PosPresTOL; c.eps0 = 0; c.sigmaMin = 0; c.sigmaMax = 0; c.ZeroTOL = std::pow(10.0, -5); c.sensor_skip = 0.0; c.ES = ES;
     switch (ngl) {
         case 2: noalloc_launch<2>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;
         case 3: noalloc_launch<3>(K, F, NumFlux, c, q, Jinv, y_xi, y_eta, x_xi, x_eta, Bx, By, Dmat, nx, ny, scal, base, L, Qt, s); break;

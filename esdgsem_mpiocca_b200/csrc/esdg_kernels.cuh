@@ -114,11 +114,12 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
     const double hL = qe[oL], huL = qe[oL + N2], hvL = qe[oL + 2 * N2];
     double hR, huR, hvR;      // right state at master node i (flux)
     double ghR, ghuR, ghvR;   // right state at node i in the right element's order (gradient)
+    const bool grad = AV && (!a.act || a.act[eL] || (eR >= 0 && a.act[eR]));
     if (eR >= 0) {
         const double* qr = a.q + (long)eR * 3 * N2;
         const int o = trace_offset(sR, ir, NGL);
         hR = qr[o]; huR = qr[o + N2]; hvR = qr[o + 2 * N2];
-        if (AV) {
+        if (grad) {
             const int o2 = trace_offset(sR, i, NGL);
             ghR = qr[o2]; ghuR = qr[o2 + N2]; ghvR = qr[o2 + 2 * N2];
         }
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
         const long exr = (long)f * NGL + ir;
         const int o = trace_offset(sL, ir, NGL);
         wall_ghost(a.nx[exr], a.ny[exr], qe[o], qe[o + N2], qe[o + 2 * N2], hR, huR, hvR);
-        if (AV) { ghR = hL; ghuR = huL; ghvR = hvL; }
+        if (grad) { ghR = hL; ghuR = huL; ghvR = hvL; }
     }
     double N0, N1, N2f;
     es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, a.bL[ex], a.bR[(long)f * NGL + ir], N0, N1, N2f);
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
     sp[0] = s * a.c.geomFace * N0;
     sp[NGL] = s * a.c.geomFace * N1;
     sp[2 * NGL] = s * a.c.geomFace * N2f;
-    if (AV && (!a.act || a.act[eL] || (eR >= 0 && a.act[eR]))) {
+    if (grad) {
         // okl/BR1_Gradient/calcNumFluxesGradient.okl:16-135 (the right trace
         // is taken in the right element's own order, as there).
         const double tol = a.c.PosPresTOL;
@@ -362,26 +363,13 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
     if (a.lam) warp_lambda<ElemShape<NGL>::THREADS>(lam, active && !to_list, ins, a.st);
 }
 
-// Modal energy sensor of one element (okl/ShockCapturing/ShockCapturing.okl:17-234),
-// evaluated by one thread; m = (h+b) nodal values [eta][xi], V = VdmInv
-// row-major [mode][node]; w receives the modal coefficients [mode_xi][mode_eta].
+// Tail of the modal energy sensor (okl/ShockCapturing/ShockCapturing.okl:131-227):
+// energy ratios of the highest modes from the modal coefficients w
+// [mode_xi][mode_eta], log10, and the sine ramp between sigma_min and
+// sigma_max.  Sums in the reference's order.
 template <int NGL>
-__device__ double shock_sensor(const PhysConst& c, const double* m, const double* V, double* w) {
-    // s_Q1modal[i][j] in the reference holds node (xi=i, eta=j).
+__device__ double sensor_tail(const PhysConst& c, const double* w) {
     constexpr int N = NGL - 1;
-    double M1[NGL * NGL];
-    for (int i = 0; i < NGL; ++i)
-        for (int j = 0; j < NGL; ++j) {
-            double acc = 0.0;
-            for (int l = 0; l < NGL; ++l) acc += V[i * NGL + l] * m[j * NGL + l];
-            M1[i * NGL + j] = acc;
-        }
-    for (int i = 0; i < NGL; ++i)
-        for (int j = 0; j < NGL; ++j) {
-            double acc = 0.0;
-            for (int l = 0; l < NGL; ++l) acc += M1[i * NGL + l] * V[j * NGL + l];
-            w[i * NGL + j] = acc;
-        }
     double z1 = 0, n1 = 0, z2 = 0, n2s = 0;
     for (int i = 0; i < N; ++i) z1 += w[i * NGL + N] * w[i * NGL + N] + w[N * NGL + i] * w[N * NGL + i];
     z1 += w[N * NGL + N] * w[N * NGL + N];
@@ -394,13 +382,47 @@ __device__ double shock_sensor(const PhysConst& c, const double* m, const double
         for (int j = 0; j < N; ++j) n2s += w[i * NGL + j] * w[i * NGL + j];
     const double t1 = (n1 < c.ZeroTOL) ? 0.0 : z1 / n1;
     const double t2 = (n1 < c.ZeroTOL) ? 0.0 : z2 / n2s;
-    const double sig = log10((t1 < t2) ? t2 : t1);
+    const double ratio = (t1 < t2) ? t2 : t1;
+    // exact shortcut: log10 is accurate to an ulp, so below this bound the
+    // reference's test sigmaMin >= log10(ratio) holds (NaN falls through)
+    if (ratio < c.sensor_skip) return 0.0;
+    const double sig = log10(ratio);
     if (c.sigmaMin >= sig) return 0.0;
     if (c.sigmaMax >= sig) {
         const double delta = 1.0 + sin(M_PI * (sig - 0.5 * (c.sigmaMax + c.sigmaMin)) / (c.sigmaMax - c.sigmaMin));
         return c.eps0 * 0.5 * delta;
     }
     return c.eps0;
+}
+
+// Modal transform entries of the sensor: M1[i][j] = sum_l V[i][l] m[j][l]
+// and w[i][j] = sum_l M1[i][l] V[j][l] (s_Q1modal[i][j] of the reference
+// holds node (xi=i, eta=j)); one entry per call, so that a thread per entry
+// computes exactly what the serial loops do.
+template <int NGL>
+__device__ __forceinline__ double sensor_m1(const double* V, const double* m, int i, int j) {
+    double acc = 0.0;
+    for (int l = 0; l < NGL; ++l) acc += V[i * NGL + l] * m[j * NGL + l];
+    return acc;
+}
+template <int NGL>
+__device__ __forceinline__ double sensor_w(const double* V, const double* M1, int i, int j) {
+    double acc = 0.0;
+    for (int l = 0; l < NGL; ++l) acc += M1[i * NGL + l] * V[j * NGL + l];
+    return acc;
+}
+
+// Modal energy sensor of one element (okl/ShockCapturing/ShockCapturing.okl:17-234),
+// evaluated by one thread; m = (h+b) nodal values [eta][xi], V = VdmInv
+// row-major [mode][node]; w receives the modal coefficients [mode_xi][mode_eta].
+template <int NGL>
+__device__ double shock_sensor(const PhysConst& c, const double* m, const double* V, double* w) {
+    double M1[NGL * NGL];
+    for (int i = 0; i < NGL; ++i)
+        for (int j = 0; j < NGL; ++j) M1[i * NGL + j] = sensor_m1<NGL>(V, m, i, j);
+    for (int i = 0; i < NGL; ++i)
+        for (int j = 0; j < NGL; ++j) w[i * NGL + j] = sensor_w<NGL>(V, M1, i, j);
+    return sensor_tail<NGL>(c, w);
 }
 
 // Shock sensor for every element and the per-instance maximum viscosity

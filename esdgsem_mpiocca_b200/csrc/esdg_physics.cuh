@@ -11,6 +11,9 @@ namespace esdg {
 struct PhysConst {
     double g, half_g, fourth_g, geomFace, PosPresTOL;
     double eps0, sigmaMin, sigmaMax, ZeroTOL;
+    // energy ratio below which log10(ratio) < sigmaMin holds with margin
+    // (10^sigmaMin (1 - 1e-12)): the sensor returns 0 without log10/sin
+    double sensor_skip;
     int ES;
 };
 
