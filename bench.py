@@ -163,15 +163,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="curved_lake", choices=["curved_lake", "ensemble"],
+    ap.add_argument("--workload", default="curved_lake", choices=["curved_lake", "ensemble", "serving"],
                     help="curved_lake: the headline single-mesh workload; ensemble: 256 seeded tsunami "
-                         "members batched vs one at a time")
+                         "members batched vs one at a time; serving: Poisson request streams")
+    ap.add_argument("--rates", default="10,100,1000", help="serving workload: arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=24, help="serving workload: requests per rate")
+    ap.add_argument("--hbm-gb", type=float, default=40.0, help="serving workload: HBM given to the arenas")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--alone-members", type=int, default=15,
                     help="ensemble workload: members solved one at a time for the plain-path rate")
     args = ap.parse_args()
     if args.workload == "ensemble":
         return ensemble_bench(args)
+    if args.workload == "serving":
+        return serving_bench(args)
     ws, rank, local = dist_env()
     args.warmup = max(args.warmup, 3)
 
@@ -440,6 +445,47 @@ def ensemble_bench(args):
             "attribution_batched": {"modal_full_path": attrib[0]["rate"], "modal_active_set": attrib[1]["rate"],
                                     "learned_active_set": learned["rate"], "steps": attr_steps},
             "gpu_launches": int(learned["launches"]), "clocks": learned["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def serving_bench(args):
+    """The serving configuration: Poisson streams of tsunami solves (K from
+    32^2 to 256^2, N in {3, 4}, 200-2000 steps) at several arrival rates,
+    served by the continuous-batching server (learned indicator, active
+    set) and, for the same streams, one request at a time by the plain
+    single-mesh path.  Reports p50/p99 latency and throughput of both."""
+    import torch
+    from esdgsem_mpiocca_b200 import serving
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    rates = [float(x) for x in args.rates.split(",")]
+    t0 = time.perf_counter()
+    streams = {rate: serving.make_requests(args.requests, rate, seed=1000 * rank + int(rate)) for rate in rates}
+    setup_s = time.perf_counter() - t0
+    srv = serving.Server(hbm_bytes=args.hbm_gb * 1e9, max_instances=256, device_id=local)
+    # warm-up: one small request through each arena
+    serving.serve(serving.make_requests(2, 1e6, seed=7, sizes=(32,), horizons=(5, 5)), srv, realtime=False)
+    out = []
+    with Clocks(local) as ck:
+        for rate in rates:
+            b = serving.serve(serving.fresh(streams[rate]), srv, realtime=True)
+            a = serving.serve_one_at_a_time(serving.fresh(streams[rate]), indicator=0, device_id=local)
+            out.append({"rate_per_s": rate, "batched": b, "plain_one_at_a_time": a,
+                        "throughput_ratio": b["throughput_dof_stages_per_s"] / a["throughput_dof_stages_per_s"],
+                        "p99_ratio": a["p99_s"] / b["p99_s"]})
+    srv.close()
+    top = out[-1]["batched"]
+    line = {"metric": METRIC, "value": top["throughput_dof_stages_per_s"] * ws, "unit": UNIT, "n_gpus": ws,
+            "steps": None, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (indicator network: bf16 weights, fp32 accumulation)",
+            "data": "synthetic (seeded tsunami requests, Poisson arrivals)",
+            "config": {"workload": f"serving: {args.requests} requests per rate, K in 32^2..256^2, N in {{3,4}}, "
+                                   "200-2000 steps, continuous batching with admission by HBM footprint "
+                                   f"({args.hbm_gb} GB of arenas), learned indicator + active set",
+                       "setup_s": setup_s, "value_is": f"batched throughput at {rates[-1]} requests/s"},
+            "rates": out, "clocks": ck.result}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

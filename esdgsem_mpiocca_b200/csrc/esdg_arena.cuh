@@ -80,7 +80,7 @@ class Arena : public Engine {
         max_inst = maxI;
         K_cap = Kc;
         F_cap = Fc;
-        if ((r = alloc(&elem_inst, (size_t)Ka))) return r;
+        if ((r = alloc(&elem_inst, (size_t)Ka)) || (r = alloc(&extent, 2))) return r;  // extent {0, 0}: none live
         st_h.assign(I, DevState{});
         for (auto& s : st_h) { std::memset(&s, 0, sizeof s); s.done = 1; s.T = 0; }
         cudaError_t e = cudaMemcpy(st, st_h.data(), sizeof(DevState) * I, cudaMemcpyHostToDevice);
@@ -191,6 +191,24 @@ class Arena : public Engine {
         inst[slot].K = K_;
         inst[slot].F = F_;
         *id = slot;
+        return update_extent();
+    }
+
+    // Highest live element and face (+1), read by the main kernels so that a
+    // sparsely filled arena costs what its live part costs.
+    int ext_h[2] = {0, 0};
+    int update_extent() {
+        int ke = 0, kf = 0;
+        for (auto& x : inst)
+            if (x.live) {
+                ke = std::max(ke, x.e.begin + x.e.size);
+                kf = std::max(kf, x.f.begin + x.f.size);
+            }
+        ext_h[0] = ke;
+        ext_h[1] = kf;
+        cudaError_t e = cudaMemcpyAsync(extent, ext_h, sizeof(ext_h), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "arena extent");
         return 0;
     }
 
@@ -226,7 +244,7 @@ class Arena : public Engine {
         give(free_e, in.e);
         give(free_f, in.f);
         in = Inst{};
-        return 0;
+        return update_extent();
     }
 
     int poll_all() {

@@ -142,6 +142,7 @@ class Engine {
     int* act = nullptr;                       // [K + 1]: flags, then the list length
     int* alist = nullptr;                     // [K] flagged elements of the stage
     int4* nbr = nullptr;                      // [K] face neighbours
+    int* extent = nullptr;                    // arena: live extent {elements, faces} (null: all)
     unsigned long long* ind_stats = nullptr;  // [4] decision counts
     std::vector<double> Vinv_h;
     int list_grid = 0;                        // persistent grid of the list kernels
@@ -186,7 +187,7 @@ class Engine {
         bytes = 0;
         if (st_host) { cudaFreeHost(st_host); st_host = nullptr; }
         q = gRK = Qt = Qtmp = nullptr;
-        mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr; nbr = nullptr;
+        mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr; nbr = nullptr; extent = nullptr;
         indicator = 0;
         inited = copied = built = false;
     }
@@ -357,6 +358,7 @@ class Engine {
     int launch_face(bool av_grad) {
         FaceArgs a{F, ftab, q, nx, ny, scal, bL, bR, SP, SGX, SGY, elem_inst, st, phys()};
         a.act = (AV && indicator) ? act : nullptr;
+        a.extent = extent;
         const long n = (long)F * NGL;
         const int blocks = (int)((n + 255) / 256);
         if (av_grad) {
@@ -378,7 +380,7 @@ class Engine {
         a.B = B; a.D = D; a.Dhat = Dhat; a.Dstrong = Dstrong; a.Vinv = Vinv; a.SP = SP; a.SGX = SGX; a.SGY = SGY;
         a.SPV = SPV; a.side = side; a.q = q; a.gRK = gRK; a.Qt = Qt; a.Qtmp = Qtmp; a.GX = GX; a.GY = GY; a.VP = VP;
         a.elem_inst = elem_inst; a.st = st; a.rkA = A; a.rkB = Bc; a.rkC = C; a.mode = mode; a.lam = lam;
-        a.shock = shock; a.c = phys();
+        a.shock = shock; a.c = phys(); a.extent = extent;
         return a;
     }
 
@@ -434,7 +436,7 @@ class Engine {
             k_grad_list<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
             const long n = (long)F * NGL;
             k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
-                                                                         elem_inst, st, geomFace, act);
+                                                                         elem_inst, st, geomFace, act, extent);
             k_element_av2<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
             launches += 3;
         } else if (!AV) {
@@ -476,7 +478,7 @@ class Engine {
         ia.K = K; ia.q = q; ia.B = B; ia.Vinv = Vinv; ia.VP = VP; ia.act = act; ia.nbr = nbr;
         ia.elem_inst = elem_inst; ia.st = st; ia.c = phys(); ia.stage0 = stage0;
         ia.P = mlpP; ia.Pb = mlpPb; ia.L = mlp_layout(NGL); ia.margin = ind_margin;
-        ia.emin = ind_emin; ia.emax = ind_emax; ia.stats = ind_stats;
+        ia.emin = ind_emin; ia.emax = ind_emax; ia.stats = ind_stats; ia.extent = extent;
         using S = IndShape<NGL>;
         const int ntiles = (K + S::NE - 1) / S::NE;
         if (indicator == 2)

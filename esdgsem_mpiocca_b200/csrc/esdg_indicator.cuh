@@ -38,6 +38,7 @@ struct IndArgs {
     double* __restrict__ VP;
     int* act;
     const int4* __restrict__ nbr;  // face neighbours (k_build_nbr)
+    const int* __restrict__ extent = nullptr;  // live extent ([0] elements), as in FaceArgs
     const int* __restrict__ elem_inst;
     DevState* st;
     PhysConst c;
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
         return;  // more elements per block than one MMA tile: never launched (N >= 3 only)
     }
     constexpr int NEL = LEARNED ? NE : 1;  // sized for the learned path only
+    if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     // an element's nodes form an aligned group of lanes (N2 divides 32)
     constexpr bool GROUP = (32 % N2) == 0;
     __shared__ double sV[N2];
@@ -155,11 +157,24 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
     if (tid < N2) sV[tid] = a.Vinv[tid];
     if (LEARNED) mlp_stage_weights(KP, a.Pb, a.L, sW1, sW2);
     unsigned long long cnt[4] = {0, 0, 0, 0};
+    // loads run PF tiles ahead: enough bytes in flight per SM to cover the
+    // memory latency at a few blocks per SM
+    constexpr int PF = LEARNED ? 2 : 3;
     int t = blockIdx.x;
-    IndLoad cur = (t < ntiles) ? ind_load<NGL, LEARNED>(a, t) : IndLoad{};
+    IndLoad ring[PF];
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+        const int tk = t + k * gridDim.x;
+        ring[k] = (tk < ntiles) ? ind_load<NGL, LEARNED>(a, tk) : IndLoad{};
+    }
     for (; t < ntiles; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        const IndLoad nxt = (tn < ntiles) ? ind_load<NGL, LEARNED>(a, tn) : IndLoad{};
+        const IndLoad cur = ring[0];
+#pragma unroll
+        for (int k = 0; k + 1 < PF; ++k) ring[k] = ring[k + 1];
+        {
+            const int tn = t + PF * gridDim.x;
+            ring[PF - 1] = (tn < ntiles) ? ind_load<NGL, LEARNED>(a, tn) : IndLoad{};
+        }
         const int e = t * NE + el;
         const bool live = e < a.K && !a.st[cur.ins].done;
         seta[s] = cur.b + cur.h;
@@ -314,7 +329,6 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
             if (!(v <= 0.0)) cnt[3] += 1;
         }
         __syncthreads();  // shared tiles are rewritten next iteration
-        cur = nxt;
     }
     if (a.stats && nd == 0) {
 #pragma unroll

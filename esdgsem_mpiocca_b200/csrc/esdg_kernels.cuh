@@ -49,6 +49,9 @@ struct FaceArgs {
     // active set (null: every face): gradient fluxes only where an adjacent
     // element is flagged
     const int* __restrict__ act = nullptr;
+    // live extent (null: all): [0] elements, [1] faces below which every
+    // live entity lies (the arena keeps it current between replays)
+    const int* __restrict__ extent = nullptr;
 };
 
 struct ElemArgs {
@@ -90,6 +93,7 @@ struct ElemArgs {
     const int* __restrict__ act = nullptr;
     int* alist = nullptr;
     int* acount = nullptr;
+    const int* __restrict__ extent = nullptr;  // live extent, as in FaceArgs
 };
 
 __device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return elem_inst ? elem_inst[e] : 0; }
@@ -102,6 +106,7 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
     const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long)a.F * NGL) return;
     const int f = (int)(gid / NGL), i = (int)(gid % NGL);
+    if (a.extent && f >= a.extent[1]) return;
     constexpr int N2 = NGL * NGL;
     const int4 t = a.ftab[f];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
@@ -163,11 +168,13 @@ __global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict
                                                    const double* __restrict__ GX, const double* __restrict__ GY,
                                                    const double* __restrict__ VP, double* __restrict__ SPV,
                                                    const int* __restrict__ elem_inst, const DevState* __restrict__ st,
-                                                   double geomFace, const int* __restrict__ act = nullptr) {
+                                                   double geomFace, const int* __restrict__ act = nullptr,
+                                                   const int* __restrict__ extent = nullptr) {
     const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long)F * NGL) return;
     constexpr int N2 = NGL * NGL;
     const int f = (int)(gid / NGL), i = (int)(gid % NGL);
+    if (extent && f >= extent[1]) return;
     const int4 t = ftab[f];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
     if (st[inst_of(elem_inst, eL)].done) return;
@@ -256,6 +263,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
     const int tid = threadIdx.x;
     const int el = tid / N2, nd = tid % N2;
     const int e0 = blockIdx.x * NE;
+    if (a.extent && e0 >= a.extent[0]) return;  // whole block past the live extent
     const int e = e0 + el;
     const bool inb = e < a.K;
     const int ins = inb ? inst_of(a.elem_inst, e) : 0;

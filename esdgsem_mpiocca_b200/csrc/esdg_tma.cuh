@@ -151,6 +151,7 @@ template <int NGL>
 __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, ESDG_TMA_MIN_BLOCKS) k_element_tma(ElemArgs a, int ntiles) {
     using S = TmaShape<NGL>;
     constexpr int N2 = S::N2, NE = S::NE, ST = S::STAGES;
+    if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     extern __shared__ __align__(128) double smem[];
     double* stage = smem;
     double* su = smem + ST * S::STAGE_DOUBLES;
