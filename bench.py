@@ -248,6 +248,7 @@ def main():
                                "achieved": STAGE_BYTES_PER_NODE * prob.dofs() * STAGES * args.steps /
                                (ms_max / 1e3) / 1e9}},
         "e2e": e2e,
+        "autotuned": s.dc.tuned_config(),
         "gpu_launches": int(launches),
         "clocks": ck.result,
     }

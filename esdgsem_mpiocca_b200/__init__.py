@@ -62,6 +62,8 @@ def _declare(lib):
         "esdg_ensemble_add": (_I, [_VP, _I, _I] + [_PD] * 13 + [_PI] * 4 + [_D, _I, _D, _D, _D, _PI]),
         "esdg_ensemble_remove": (_I, [_VP, _I]),
         "esdg_ensemble_advance": (_I, [_VP, _I]),
+        "esdg_ensemble_launch": (_I, [_VP, _I]),
+        "esdg_ensemble_sync": (_I, [_VP]),
         "esdg_ensemble_status": (_I, [_VP, _I, _PD, _PI, _PI, _PI]),
         "esdg_ensemble_copy_q": (_I, [_VP, _I, _PD]),
         "esdg_ensemble_free_capacity": (_I, [_VP, _PI, _PI, _PI]),
@@ -71,6 +73,7 @@ def _declare(lib):
         "esdg_ensemble_last_error": (ctypes.c_char_p, [_VP]),
         "esdg_ensemble_destroy": (_I, [_VP]),
         "esdg_state_pointers": (_I, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+        "esdg_tuned_config": (_I, [_VP, _PI, ctypes.POINTER(ctypes.c_float)]),
         "esdg_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),
         "esdg_indicator_stats": (_I, [_VP, ctypes.POINTER(ctypes.c_ulonglong), _I]),
         "esdg_ensemble_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),

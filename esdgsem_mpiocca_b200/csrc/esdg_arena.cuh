@@ -255,12 +255,25 @@ class Arena : public Engine {
     }
 
     int advance_arena(int nsteps) {
+        int r = launch_arena(nsteps);
+        return r ? r : poll_all();
+    }
+
+    // Replays the step graph nsteps times without waiting.
+    int launch_arena(int nsteps) {
+        if (!tma_tuned && ext_h[0] > 0) {
+            // tune on the first live contents, then re-capture with the choice
+            const int before = tma_variant;
+            int r = run_autotune();
+            if (r) return r;
+            if (tma_variant != before && (r = capture_step_graph())) return r;
+        }
         for (int k = 0; k < nsteps; ++k) {
             cudaError_t e = cudaGraphLaunch(graph, stream);
             if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
             launches += kernels_per_step;
         }
-        return poll_all();
+        return 0;
     }
 
     int copy_q_inst(int id, double* qh) {
@@ -338,6 +351,18 @@ int esdg_ensemble_advance(esdg_ensemble* en, int nsteps) {
     if (!en || nsteps < 0) return ESDG_E_ARG;
     cudaSetDevice(en->a.device);
     return en->a.advance_arena(nsteps);
+}
+
+int esdg_ensemble_launch(esdg_ensemble* en, int nsteps) {
+    if (!en || nsteps < 0) return ESDG_E_ARG;
+    cudaSetDevice(en->a.device);
+    return en->a.launch_arena(nsteps);
+}
+
+int esdg_ensemble_sync(esdg_ensemble* en) {
+    if (!en) return ESDG_E_ARG;
+    cudaSetDevice(en->a.device);
+    return en->a.poll_all();
 }
 
 int esdg_ensemble_status(esdg_ensemble* en, int id, double* t, int* steps, int* done, int* status) {

@@ -386,36 +386,98 @@ class Engine {
 
     // Plain-path element kernel: the TMA-pipelined persistent kernel when the
     // element count allows 16-byte bulk granularity, else the one-shot one.
-    int tma_grid = 0;  // persistent grid size (0: not set up / not usable)
+    // Its occupancy variant (tma_min_blocks) is picked by timing on the mesh.
+    int tma_grid[TMA_VARIANTS] = {0, 0};  // persistent grid sizes (0: not usable)
+    int tma_variant = 0;
+    bool tma_tuned = false;
+    float tma_tune_ms[TMA_VARIANTS] = {0.0f, 0.0f};
 
-    template <int NGL>
-    int setup_tma() {
+    template <int NGL, int V>
+    int setup_tma_variant() {
         using T = TmaShape<NGL>;
-        tma_grid = 0;
-        if (((long long)K * T::N2) % 2 != 0) return 0;
-        cudaError_t e = cudaFuncSetAttribute(k_element_tma<NGL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)T::SMEM);
+        auto kern = k_element_tma<NGL, tma_min_blocks(V)>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0, sms = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_element_tma<NGL>, T::THREADS, T::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T::THREADS, T::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
         const int ntiles = (K + T::NE - 1) / T::NE;
-        tma_grid = std::max(1, std::min(ntiles, std::max(per_sm, 1) * sms));
+        tma_grid[V] = std::max(1, std::min(ntiles, std::max(per_sm, 1) * sms));
         return 0;
     }
 
     template <int NGL>
+    int setup_tma() {
+        using T = TmaShape<NGL>;
+        tma_grid[0] = tma_grid[1] = 0;
+        tma_tuned = false;
+        tma_variant = 0;
+        if (((long long)K * T::N2) % 2 != 0) return 0;
+        int r = setup_tma_variant<NGL, 0>();
+        if (!r) r = setup_tma_variant<NGL, 1>();
+        return r;
+    }
+
+    template <int NGL>
+    void launch_tma(const ElemArgs& ea, int v) {
+        using T = TmaShape<NGL>;
+        const int ntiles = (K + T::NE - 1) / T::NE;
+        if (v == 0)
+            k_element_tma<NGL, tma_min_blocks(0)><<<tma_grid[0], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+        else
+            k_element_tma<NGL, tma_min_blocks(1)><<<tma_grid[1], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+    }
+
+    template <int NGL>
     void launch_elem_plain(const ElemArgs& ea) {
-        if (tma_grid > 0) {
-            using T = TmaShape<NGL>;
-            k_element_tma<NGL><<<tma_grid, T::THREADS, T::SMEM, stream>>>(ea, (K + T::NE - 1) / T::NE);
+        if (tma_grid[tma_variant] > 0) {
+            launch_tma<NGL>(ea, tma_variant);
         } else {
             using S = ElemShape<NGL>;
             k_element<NGL><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, stream>>>(ea);
         }
         ++launches;
+    }
+
+    // Autotuner: times every occupancy variant of the element kernel on this
+    // mesh (mode 2: only Qt is written, the state is untouched) and keeps
+    // the fastest; runs once, before the step graph is captured.
+    template <int NGL>
+    int autotune_tma() {
+        if (tma_tuned) return 0;
+        tma_tuned = true;
+        if (tma_grid[0] <= 0) return 0;
+        cudaEvent_t ev[2];
+        if (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess)
+            return fail(ESDG_E_CUDA, "cudaEventCreate");
+        ElemArgs ea = elem_args(2, 0.0, 0.0, 0.0, 0, 0);
+        ea.extent = nullptr;
+        float best = 1e30f;
+        for (int v = 0; v < TMA_VARIANTS; ++v) {
+            if (tma_grid[v] <= 0) continue;
+            for (int k = 0; k < 2; ++k) launch_tma<NGL>(ea, v);  // warm-up
+            cudaEventRecord(ev[0], stream);
+            for (int k = 0; k < 5; ++k) launch_tma<NGL>(ea, v);
+            cudaEventRecord(ev[1], stream);
+            cudaError_t e = cudaEventSynchronize(ev[1]);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            if (e != cudaSuccess) {
+                cudaEventDestroy(ev[0]);
+                cudaEventDestroy(ev[1]);
+                return cuda_fail(e, "autotune");
+            }
+            tma_tune_ms[v] = ms / 5.0f;
+            if (tma_tune_ms[v] < best) {
+                best = tma_tune_ms[v];
+                tma_variant = v;
+            }
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        return 0;
     }
 
     template <int NGL>
@@ -618,6 +680,19 @@ class Engine {
         return 0;
     }
 
+    int run_autotune() {
+        switch (ngl) {
+            case 2: return autotune_tma<2>();
+            case 3: return autotune_tma<3>();
+            case 4: return autotune_tma<4>();
+            case 5: return autotune_tma<5>();
+            case 6: return autotune_tma<6>();
+            case 7: return autotune_tma<7>();
+            case 8: return autotune_tma<8>();
+        }
+        return 0;
+    }
+
     int capture_step_graph() {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         const long long before = launches;
@@ -682,6 +757,7 @@ class Engine {
         if (e != cudaSuccess) return cuda_fail(e, "state upload");
         ESDG_DISPATCH(ngl, launch_bottom);
         ESDG_DISPATCH(ngl, launch_lambda);
+        if ((r = run_autotune())) return r;
         if ((r = capture_step_graph())) return r;
         if ((r = run_steps(max_steps > 0 ? max_steps : 0))) return r;
         if ((r = poll_state())) return r;
@@ -1010,6 +1086,15 @@ int esdg_indicator_stats(esdg_deviceclass* d, unsigned long long* counts4, int r
     ESDG_GUARD(d);
     if (!counts4) return d->eng.fail(ESDG_E_ARG, "null counts");
     return d->eng.indicator_stats(counts4, reset);
+}
+
+int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, float* ms_variants2) {
+    if (!d) return ESDG_E_ARG;
+    const esdg::Engine& E = d->eng;
+    if (ctas_per_sm) *ctas_per_sm = E.tma_grid[E.tma_variant] > 0 ? esdg::tma_min_blocks(E.tma_variant) : 0;
+    if (ms_variants2)
+        for (int v = 0; v < esdg::TMA_VARIANTS; ++v) ms_variants2[v] = E.tma_tune_ms[v];
+    return E.tma_tuned ? ESDG_OK : ESDG_E_ARG;
 }
 
 int esdg_state_pointers(esdg_deviceclass* d, const double** q, const double** b, const double** VdmInv) {

@@ -102,9 +102,11 @@ __device__ __forceinline__ void pair_flux_raw(double g, double hL, double huL, d
     }
 }
 
-#ifndef ESDG_TMA_MIN_BLOCKS
-#define ESDG_TMA_MIN_BLOCKS 2
-#endif
+// Occupancy variants of the element kernel (CTAs per SM the register
+// budget is cut for); the engine times them on the mesh and keeps the
+// faster one.
+constexpr int TMA_VARIANTS = 2;
+__host__ __device__ constexpr int tma_min_blocks(int v) { return v == 0 ? 2 : 3; }
 
 template <int NGL>
 struct TmaShape {
@@ -147,8 +149,8 @@ __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double*
 
 // Persistent flux-differencing volume term + surface lift + RK update
 // (same operations as k_element), tiles double-buffered through TMA.
-template <int NGL>
-__global__ void __launch_bounds__(TmaShape<NGL>::THREADS, ESDG_TMA_MIN_BLOCKS) k_element_tma(ElemArgs a, int ntiles) {
+template <int NGL, int MINB>
+__global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(ElemArgs a, int ntiles) {
     using S = TmaShape<NGL>;
     constexpr int N2 = S::N2, NE = S::NE, ST = S::STAGES;
     if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);

@@ -150,6 +150,14 @@ class DeviceClass:
         self._ok(self._L.esdg_indicator_stats(self.h, out, int(reset)))
         return dict(zip(("net_zero", "net_full", "modal", "viscous"), [int(v) for v in out]))
 
+    def tuned_config(self):
+        """Element-kernel occupancy chosen by the autotuner and the measured
+        launch times of the variants (ms)."""
+        c = ctypes.c_int()
+        ms = (ctypes.c_float * 2)()
+        rc = self._L.esdg_tuned_config(self.h, ctypes.byref(c), ms)
+        return None if rc != 0 else {"ctas_per_sm": c.value, "variant_ms": [float(v) for v in ms]}
+
     def state_pointers(self):
         """Device addresses (q, b, VdmInv) of the engine's own buffers."""
         q, b, v = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()

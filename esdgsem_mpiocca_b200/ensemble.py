@@ -65,6 +65,13 @@ class Ensemble:
     def advance(self, nsteps: int):
         self._ok(self._L.esdg_ensemble_advance(self.h, nsteps))
 
+    def launch(self, nsteps: int):
+        """advance() without waiting; sync() waits and refreshes status."""
+        self._ok(self._L.esdg_ensemble_launch(self.h, nsteps))
+
+    def sync(self):
+        self._ok(self._L.esdg_ensemble_sync(self.h))
+
     def status(self, i: int):
         t, s, d, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._ok(self._L.esdg_ensemble_status(self.h, i, ctypes.byref(t), ctypes.byref(s), ctypes.byref(d),

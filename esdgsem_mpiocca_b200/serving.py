@@ -141,10 +141,12 @@ class Server:
         """Advances every arena with live requests by `chunk` steps and
         retires the finished ones (results copied out, capacity freed)."""
         done = []
-        for N, en in self.arenas.items():
-            if not self.live[N]:
-                continue
-            en.advance(self.chunk)
+        running = [N for N in self.arenas if self.live[N]]
+        for N in running:  # the arenas run concurrently, each on its own stream
+            self.arenas[N].launch(self.chunk)
+        for N in running:
+            en = self.arenas[N]
+            en.sync()
             for i in list(self.live[N]):
                 s = en.status(i)
                 if s["done"]:

@@ -152,6 +152,14 @@ int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES, double g_
                              const int* ElemEdgeMasterSlave, const int* ElemEdgeOrientation, double* Qt,
                              void* stream);
 
+/* Element-kernel occupancy chosen by the engine's autotuner (no
+ * counterpart in the reference): before the first step graph is captured the
+ * engine times each compiled occupancy variant of the element kernel on the
+ * mesh (writing only Qt) and keeps the fastest.  *ctas_per_sm receives the
+ * chosen CTAs per SM (0: the one-shot kernel is used), ms_variants2 [2] (may
+ * be NULL) the measured launch times.  ESDG_E_ARG before the tuning ran. */
+int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, float* ms_variants2);
+
 /* Device addresses of the solution q [K][3][(N+1)^2], the bathymetry b
  * [K][(N+1)^2] and VdmInv [(N+1)^2] owned by the engine (no counterpart in
  * the reference), for device-side consumers such as the indicator's
@@ -217,6 +225,13 @@ int esdg_ensemble_remove(esdg_ensemble* en, int id);
 /* Replays the step graph nsteps times (finished instances are skipped on
  * the device) and refreshes the host copy of every instance's status. */
 int esdg_ensemble_advance(esdg_ensemble* en, int nsteps);
+
+/* The two halves of esdg_ensemble_advance: replay the step graph nsteps
+ * times on the ensemble's stream without waiting, and wait for it and
+ * refresh the host status -- so that several ensembles (one per degree) run
+ * concurrently. */
+int esdg_ensemble_launch(esdg_ensemble* en, int nsteps);
+int esdg_ensemble_sync(esdg_ensemble* en);
 
 /* Status from the last advance: time, steps taken, done flag, status
  * (0 ok, 1 non-finite wave speed). */
