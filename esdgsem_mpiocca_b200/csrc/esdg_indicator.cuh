@@ -127,7 +127,7 @@ __device__ __forceinline__ IndLoad ind_load(const IndArgs& a, int t) {
 // Persistent: each block walks tiles of NE elements, the next tile's loads
 // in flight while the current one is processed.
 template <int NGL, bool LEARNED>
-__global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a, int ntiles) {
+__global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs a, int ntiles) {
     using S = IndShape<NGL>;
     constexpr int N2 = S::N2, NE = S::NE, KP = S::KP;
     if constexpr (LEARNED && NE > S::ROWS) {
@@ -147,8 +147,6 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
     __shared__ __align__(32) __nv_bfloat16 sX[LEARNED ? S::ROWS * KP : 16];
     __shared__ __align__(32) __nv_bfloat16 sW1[LEARNED ? MLP_H * KP : 16];
     __shared__ __align__(32) __nv_bfloat16 sW2[LEARNED ? MLP_H * MLP_H : 16];
-    __shared__ __align__(32) __nv_bfloat16 a1b[LEARNED ? 16 * 32 : 16];
-    __shared__ __align__(32) float zs[LEARNED ? 16 * 32 : 16];
     __shared__ float y16[16];
 
     const int tid = threadIdx.x;
@@ -159,7 +157,7 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
     unsigned long long cnt[4] = {0, 0, 0, 0};
     // loads run PF tiles ahead: enough bytes in flight per SM to cover the
     // memory latency at a few blocks per SM
-    constexpr int PF = LEARNED ? 2 : 3;
+    constexpr int PF = LEARNED ? 1 : 2;
     int t = blockIdx.x;
     IndLoad ring[PF];
 #pragma unroll
@@ -224,7 +222,14 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
                 if (r >= NE || t * NE + r >= a.K || c >= 3 * N2 + 3) sX[i] = __float2bfloat16(0.0f);
             }
             __syncthreads();
-            if (tid < 32) mlp_warp_forward<KP>(sX, sW1, sW2, a.P, a.L, a1b, zs, y16);
+            if (tid < 32) {
+                float ylo, yhi;
+                mlp_warp_forward_regs<KP>(sX, sW1, sW2, a.P, a.L, ylo, yhi);
+                if ((tid & 3) == 0) {
+                    y16[tid >> 2] = ylo;
+                    y16[(tid >> 2) + 8] = yhi;
+                }
+            }
             __syncthreads();
             if (live && nd == 0) need[el] = learned_needs_modal(a, (double)y16[el] + fs_eta[el], fE[el] * N2, fok[el]);
         } else if (LEARNED) {
@@ -271,7 +276,14 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_indicator(IndArgs a,
                 }
             }
             __syncthreads();
-            if (tid < 32) mlp_warp_forward<KP>(sX, sW1, sW2, a.P, a.L, a1b, zs, y16);
+            if (tid < 32) {
+                float ylo, yhi;
+                mlp_warp_forward_regs<KP>(sX, sW1, sW2, a.P, a.L, ylo, yhi);
+                if ((tid & 3) == 0) {
+                    y16[tid >> 2] = ylo;
+                    y16[(tid >> 2) + 8] = yhi;
+                }
+            }
             __syncthreads();
             if (live && nd == 0) need[el] = learned_needs_modal(a, (double)y16[el] + fs_eta[el], fE[el] * N2, fok[el]);
         }

@@ -236,6 +236,94 @@ __device__ __forceinline__ void mlp_warp_forward(const __nv_bfloat16* Xrows, con
     __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// Forward pass on registers: mma.sync.m16n8k16 (BF16 in, FP32 accumulate)
+// with the PTX ISA fragment layouts -- lane = 4 g + t; A (16x16, row):
+// a0 (g, 2t..2t+1), a1 (g+8, 2t..), a2 (g, 2t+8..), a3 (g+8, 2t+8..);
+// B (16x8, col): b0 (k 2t..2t+1, n g), b1 (k 2t+8..2t+9, n g);
+// C (16x8): c0,c1 (g, 2t..2t+1), c2,c3 (g+8, 2t..2t+1).  Layer-1 outputs
+// of two adjacent n8 tiles form the layer-2 A fragment of one k16 block, so
+// bias, ReLU and the BF16 packing stay in registers; the 32 -> 1 layer is a
+// per-lane partial dot product reduced over the four lanes of a quad.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned mlp_pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x = lo (low half)
+    return *reinterpret_cast<const unsigned*>(&v);
+}
+
+__device__ __forceinline__ void mlp_mma16816(float (&c)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
+                                             unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// y for the 16 rows of X (bf16, shared, ld KP): lanes with t == 0 hold
+// y[g] in y_lo and y[g + 8] in y_hi (every lane of the quad has them).
+// W1 [32][KP], W2 [32][32] bf16 in shared memory; P the FP32 block.
+template <int KP>
+__device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, const __nv_bfloat16* W1,
+                                                      const __nv_bfloat16* W2, const float* __restrict__ P,
+                                                      const MlpLayout& L, float& y_lo, float& y_hi) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const unsigned* Xu = reinterpret_cast<const unsigned*>(X);    // pairs of bf16
+    const unsigned* W1u = reinterpret_cast<const unsigned*>(W1);
+    const unsigned* W2u = reinterpret_cast<const unsigned*>(W2);
+    float acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float b0 = P[L.b1 + 8 * j + 2 * t], b1v = P[L.b1 + 8 * j + 2 * t + 1];
+        acc[j][0] = b0; acc[j][1] = b1v; acc[j][2] = b0; acc[j][3] = b1v;
+    }
+#pragma unroll
+    for (int kb = 0; kb < KP / 16; ++kb) {
+        const int c = kb * 8 + t;  // column pair index (2 bf16 per unsigned)
+        const unsigned a0 = Xu[g * (KP / 2) + c], a1 = Xu[(g + 8) * (KP / 2) + c];
+        const unsigned a2 = Xu[g * (KP / 2) + c + 4], a3 = Xu[(g + 8) * (KP / 2) + c + 4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = 8 * j + g;  // B(k, n) = W1[n][k]
+            mlp_mma16816(acc[j], a0, a1, a2, a3, W1u[n * (KP / 2) + c], W1u[n * (KP / 2) + c + 4]);
+        }
+    }
+    float acc2[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float b0 = P[L.b2 + 8 * j + 2 * t], b1v = P[L.b2 + 8 * j + 2 * t + 1];
+        acc2[j][0] = b0; acc2[j][1] = b1v; acc2[j][2] = b0; acc2[j][3] = b1v;
+    }
+#pragma unroll
+    for (int kb = 0; kb < 2; ++kb) {
+        // A1 k16 block kb = layer-1 n8 tiles 2 kb and 2 kb + 1, after ReLU
+        const int j0 = 2 * kb, j1 = 2 * kb + 1;
+        const unsigned a0 = mlp_pack_bf16(fmaxf(acc[j0][0], 0.f), fmaxf(acc[j0][1], 0.f));
+        const unsigned a1 = mlp_pack_bf16(fmaxf(acc[j0][2], 0.f), fmaxf(acc[j0][3], 0.f));
+        const unsigned a2 = mlp_pack_bf16(fmaxf(acc[j1][0], 0.f), fmaxf(acc[j1][1], 0.f));
+        const unsigned a3 = mlp_pack_bf16(fmaxf(acc[j1][2], 0.f), fmaxf(acc[j1][3], 0.f));
+        const int c = kb * 8 + t;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = 8 * j + g;  // B(k, n) = W2[n][k]
+            mlp_mma16816(acc2[j], a0, a1, a2, a3, W2u[n * 16 + c], W2u[n * 16 + c + 4]);
+        }
+    }
+    float lo = 0.f, hi = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float w0 = P[L.w3 + 8 * j + 2 * t], w1 = P[L.w3 + 8 * j + 2 * t + 1];
+        lo += fmaxf(acc2[j][0], 0.f) * w0 + fmaxf(acc2[j][1], 0.f) * w1;
+        hi += fmaxf(acc2[j][2], 0.f) * w0 + fmaxf(acc2[j][3], 0.f) * w1;
+    }
+    lo += __shfl_xor_sync(0xffffffffu, lo, 1);
+    lo += __shfl_xor_sync(0xffffffffu, lo, 2);
+    hi += __shfl_xor_sync(0xffffffffu, hi, 1);
+    hi += __shfl_xor_sync(0xffffffffu, hi, 2);
+    y_lo = lo + P[L.b3];
+    y_hi = hi + P[L.b3];
+}
+
 // Shared-memory carve-up of the MLP kernels (bytes): the BF16 weights once
 // per block, then per warp: X tile, A1 (bf16), Z (float), dZ2 and dZ1
 // (bf16), scratch (float), y.
@@ -296,10 +384,16 @@ __global__ void __launch_bounds__(128) k_mlp_forward(int M, const __nv_bfloat16*
     for (int t = blockIdx.x * 4 + w; t < tiles; t += gridDim.x * 4) {
         const int r0 = t * 16;
         mlp_load_rows<KP>(X, M, r0, sX);
-        mlp_warp_forward<KP>(sX, sW1, sW2, P, L, a1b, z, y16);
-        if (lane < 16 && r0 + lane < M) y[r0 + lane] = y16[lane];
+        float ylo, yhi;
+        mlp_warp_forward_regs<KP>(sX, sW1, sW2, P, L, ylo, yhi);
+        const int g = lane >> 2;
+        if ((lane & 3) == 0) {
+            if (r0 + g < M) y[r0 + g] = ylo;
+            if (r0 + g + 8 < M) y[r0 + g + 8] = yhi;
+        }
         __syncwarp();
     }
+    (void)a1b; (void)z; (void)y16;
 }
 
 // Gradient of the loss (1/M) sum (y - t)^2 over M rows.  Each warp
