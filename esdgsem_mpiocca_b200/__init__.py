@@ -73,7 +73,7 @@ def _declare(lib):
         "esdg_ensemble_last_error": (ctypes.c_char_p, [_VP]),
         "esdg_ensemble_destroy": (_I, [_VP]),
         "esdg_state_pointers": (_I, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
-        "esdg_tuned_config": (_I, [_VP, _PI, ctypes.POINTER(ctypes.c_float)]),
+        "esdg_tuned_config": (_I, [_VP, _PI, _PI, ctypes.POINTER(ctypes.c_float)]),
         "esdg_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),
         "esdg_indicator_stats": (_I, [_VP, ctypes.POINTER(ctypes.c_ulonglong), _I]),
         "esdg_ensemble_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),

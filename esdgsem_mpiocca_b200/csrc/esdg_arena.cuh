@@ -264,6 +264,7 @@ class Arena : public Engine {
         if (!tma_tuned && ext_h[0] > 0) {
             // tune on the first live contents, then re-capture with the choice
             const int before = tma_variant;
+            tune_K = ext_h[0];
             int r = run_autotune();
             if (r) return r;
             if (tma_variant != before && (r = capture_step_graph())) return r;

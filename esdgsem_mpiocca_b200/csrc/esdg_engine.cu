@@ -387,15 +387,15 @@ class Engine {
     // Plain-path element kernel: the TMA-pipelined persistent kernel when the
     // element count allows 16-byte bulk granularity, else the one-shot one.
     // Its occupancy variant (tma_min_blocks) is picked by timing on the mesh.
-    int tma_grid[TMA_VARIANTS] = {0, 0};  // persistent grid sizes (0: not usable)
+    int tma_grid[TMA_VARIANTS] = {0, 0, 0};  // persistent grid sizes (0: not usable)
     int tma_variant = 0;
     bool tma_tuned = false;
-    float tma_tune_ms[TMA_VARIANTS] = {0.0f, 0.0f};
+    float tma_tune_ms[TMA_VARIANTS] = {0.0f, 0.0f, 0.0f};
 
     template <int NGL, int V>
     int setup_tma_variant() {
-        using T = TmaShape<NGL>;
-        auto kern = k_element_tma<NGL, tma_min_blocks(V)>;
+        using T = TmaShape<NGL, tma_stages(V)>;
+        auto kern = k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0, sms = 0;
@@ -411,23 +411,28 @@ class Engine {
     template <int NGL>
     int setup_tma() {
         using T = TmaShape<NGL>;
-        tma_grid[0] = tma_grid[1] = 0;
+        for (auto& g : tma_grid) g = 0;
         tma_tuned = false;
         tma_variant = 0;
         if (((long long)K * T::N2) % 2 != 0) return 0;
         int r = setup_tma_variant<NGL, 0>();
         if (!r) r = setup_tma_variant<NGL, 1>();
+        if (!r) r = setup_tma_variant<NGL, 2>();
         return r;
+    }
+
+    template <int NGL, int V>
+    void launch_tma_v(const ElemArgs& ea) {
+        using T = TmaShape<NGL, tma_stages(V)>;
+        const int ntiles = (K + T::NE - 1) / T::NE;
+        k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
     }
 
     template <int NGL>
     void launch_tma(const ElemArgs& ea, int v) {
-        using T = TmaShape<NGL>;
-        const int ntiles = (K + T::NE - 1) / T::NE;
-        if (v == 0)
-            k_element_tma<NGL, tma_min_blocks(0)><<<tma_grid[0], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
-        else
-            k_element_tma<NGL, tma_min_blocks(1)><<<tma_grid[1], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+        if (v == 0) launch_tma_v<NGL, 0>(ea);
+        else if (v == 1) launch_tma_v<NGL, 1>(ea);
+        else launch_tma_v<NGL, 2>(ea);
     }
 
     template <int NGL>
@@ -441,42 +446,58 @@ class Engine {
         ++launches;
     }
 
-    // Autotuner: times every occupancy variant of the element kernel on this
-    // mesh (mode 2: only Qt is written, the state is untouched) and keeps
-    // the fastest; runs once, before the step graph is captured.
+    // Autotuner: times every variant of the element kernel on this mesh in
+    // the step's own update mode, on copies of q and gRK (the state is not
+    // touched), and keeps the fastest; runs once, before the step graph is
+    // captured.  tune_K: elements to cover (the arena's live extent).
+    int tune_K = -1;
+
     template <int NGL>
     int autotune_tma() {
         if (tma_tuned) return 0;
         tma_tuned = true;
         if (tma_grid[0] <= 0) return 0;
+        const int Kt = tune_K >= 0 ? tune_K : K;
+        if (Kt <= 0) return 0;
+        const size_t nd = (size_t)Kt * NGL * NGL * 3;
+        double *tq = nullptr, *tg = nullptr;
+        if (cudaMalloc(&tq, nd * sizeof(double)) != cudaSuccess || cudaMalloc(&tg, nd * sizeof(double)) != cudaSuccess) {
+            cudaFree(tq);
+            cudaGetLastError();
+            tma_tuned = false;  // no room for the copies: keep the default variant
+            return 0;
+        }
+        cudaMemcpyAsync(tq, q, nd * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(tg, gRK, nd * sizeof(double), cudaMemcpyDeviceToDevice, stream);
         cudaEvent_t ev[2];
-        if (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess)
-            return fail(ESDG_E_CUDA, "cudaEventCreate");
-        ElemArgs ea = elem_args(2, 0.0, 0.0, 0.0, 0, 0);
-        ea.extent = nullptr;
+        cudaEventCreate(&ev[0]);
+        cudaEventCreate(&ev[1]);
+        const bool have = gStages > 0;
+        ElemArgs ea = elem_args(rkSSP ? 1 : 0, have ? gA[0] : 0.0, have ? gB[0] : 1.0, have ? gC[0] : 0.0, 0, 0);
+        ea.q = tq;
+        ea.gRK = tg;
         float best = 1e30f;
-        for (int v = 0; v < TMA_VARIANTS; ++v) {
+        cudaError_t e = cudaSuccess;
+        for (int v = 0; v < TMA_VARIANTS && e == cudaSuccess; ++v) {
             if (tma_grid[v] <= 0) continue;
             for (int k = 0; k < 2; ++k) launch_tma<NGL>(ea, v);  // warm-up
             cudaEventRecord(ev[0], stream);
             for (int k = 0; k < 5; ++k) launch_tma<NGL>(ea, v);
             cudaEventRecord(ev[1], stream);
-            cudaError_t e = cudaEventSynchronize(ev[1]);
+            e = cudaEventSynchronize(ev[1]);
             float ms = 0.0f;
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
-            if (e != cudaSuccess) {
-                cudaEventDestroy(ev[0]);
-                cudaEventDestroy(ev[1]);
-                return cuda_fail(e, "autotune");
-            }
             tma_tune_ms[v] = ms / 5.0f;
-            if (tma_tune_ms[v] < best) {
+            if (e == cudaSuccess && tma_tune_ms[v] < best) {
                 best = tma_tune_ms[v];
                 tma_variant = v;
             }
         }
         cudaEventDestroy(ev[0]);
         cudaEventDestroy(ev[1]);
+        cudaFree(tq);
+        cudaFree(tg);
+        if (e != cudaSuccess) return cuda_fail(e, "autotune");
         return 0;
     }
 
@@ -1088,12 +1109,13 @@ int esdg_indicator_stats(esdg_deviceclass* d, unsigned long long* counts4, int r
     return d->eng.indicator_stats(counts4, reset);
 }
 
-int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, float* ms_variants2) {
+int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, int* stages, float* ms_variants2) {
     if (!d) return ESDG_E_ARG;
     const esdg::Engine& E = d->eng;
     if (ctas_per_sm) *ctas_per_sm = E.tma_grid[E.tma_variant] > 0 ? esdg::tma_min_blocks(E.tma_variant) : 0;
     if (ms_variants2)
         for (int v = 0; v < esdg::TMA_VARIANTS; ++v) ms_variants2[v] = E.tma_tune_ms[v];
+    if (stages) *stages = E.tma_grid[E.tma_variant] > 0 ? esdg::tma_stages(E.tma_variant) : 0;
     return E.tma_tuned ? ESDG_OK : ESDG_E_ARG;
 }
 

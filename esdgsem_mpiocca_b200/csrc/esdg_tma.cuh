@@ -102,20 +102,21 @@ __device__ __forceinline__ void pair_flux_raw(double g, double hL, double huL, d
     }
 }
 
-// Occupancy variants of the element kernel (CTAs per SM the register
-// budget is cut for); the engine times them on the mesh and keeps the
-// faster one.
-constexpr int TMA_VARIANTS = 2;
-__host__ __device__ constexpr int tma_min_blocks(int v) { return v == 0 ? 2 : 3; }
+// Variants of the element kernel: CTAs per SM the register budget is cut
+// for, and depth of the bulk-copy pipeline; the engine times them on the
+// mesh and keeps the fastest.
+constexpr int TMA_VARIANTS = 3;
+__host__ __device__ constexpr int tma_min_blocks(int v) { return v == 1 ? 3 : 2; }
+__host__ __device__ constexpr int tma_stages(int v) { return v == 2 ? 3 : 2; }
 
-template <int NGL>
+template <int NGL, int ST = 2>
 struct TmaShape {
     static constexpr int N2 = NGL * NGL;
     // elements per tile: ~256 threads, NE*N2 even (16-byte bulk granularity)
     static constexpr int NE0 = (256 / N2) > 0 ? (256 / N2) : 1;
     static constexpr int NE = (N2 % 2 == 1 && NE0 % 2 == 1) ? (NE0 > 1 ? NE0 - 1 : 2) : NE0;
     static constexpr int THREADS = NE * N2;
-    static constexpr int STAGES = 2;
+    static constexpr int STAGES = ST;
     static constexpr int QD = NE * 3 * N2;  // doubles of a q-like section
     static constexpr int ND = NE * N2;      // doubles of a nodal section
     static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND;
@@ -149,9 +150,9 @@ __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double*
 
 // Persistent flux-differencing volume term + surface lift + RK update
 // (same operations as k_element), tiles double-buffered through TMA.
-template <int NGL, int MINB>
+template <int NGL, int MINB, int NST>
 __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(ElemArgs a, int ntiles) {
-    using S = TmaShape<NGL>;
+    using S = TmaShape<NGL, NST>;
     constexpr int N2 = S::N2, NE = S::NE, ST = S::STAGES;
     if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     extern __shared__ __align__(128) double smem[];

@@ -153,10 +153,11 @@ class DeviceClass:
     def tuned_config(self):
         """Element-kernel occupancy chosen by the autotuner and the measured
         launch times of the variants (ms)."""
-        c = ctypes.c_int()
-        ms = (ctypes.c_float * 2)()
-        rc = self._L.esdg_tuned_config(self.h, ctypes.byref(c), ms)
-        return None if rc != 0 else {"ctas_per_sm": c.value, "variant_ms": [float(v) for v in ms]}
+        c, st = ctypes.c_int(), ctypes.c_int()
+        ms = (ctypes.c_float * 3)()
+        rc = self._L.esdg_tuned_config(self.h, ctypes.byref(c), ctypes.byref(st), ms)
+        return None if rc != 0 else {"ctas_per_sm": c.value, "stages": st.value,
+                                     "variant_ms": [float(v) for v in ms]}
 
     def state_pointers(self):
         """Device addresses (q, b, VdmInv) of the engine's own buffers."""

@@ -152,13 +152,15 @@ int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES, double g_
                              const int* ElemEdgeMasterSlave, const int* ElemEdgeOrientation, double* Qt,
                              void* stream);
 
-/* Element-kernel occupancy chosen by the engine's autotuner (no
- * counterpart in the reference): before the first step graph is captured the
- * engine times each compiled occupancy variant of the element kernel on the
- * mesh (writing only Qt) and keeps the fastest.  *ctas_per_sm receives the
- * chosen CTAs per SM (0: the one-shot kernel is used), ms_variants2 [2] (may
- * be NULL) the measured launch times.  ESDG_E_ARG before the tuning ran. */
-int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, float* ms_variants2);
+/* Element-kernel variant chosen by the engine's autotuner (no counterpart
+ * in the reference): before the first step graph is captured the engine
+ * times each compiled variant of the element kernel -- CTAs per SM the
+ * register budget is cut for (2 or 3) and bulk-copy pipeline depth (2 or 3
+ * tiles) -- on the mesh (writing only Qt) and keeps the fastest.
+ * *ctas_per_sm and *stages receive the choice (0: the one-shot kernel is
+ * used), ms_variants3 [3] (may be NULL) the measured launch times.
+ * ESDG_E_ARG before the tuning ran. */
+int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, int* stages, float* ms_variants3);
 
 /* Device addresses of the solution q [K][3][(N+1)^2], the bathymetry b
  * [K][(N+1)^2] and VdmInv [(N+1)^2] owned by the engine (no counterpart in
