@@ -142,6 +142,11 @@ class Engine {
     int* act = nullptr;                       // [K + 1]: flags, then the list length
     int* alist = nullptr;                     // [K] flagged elements of the stage
     int4* nbr = nullptr;                      // [K] face neighbours
+    __nv_bfloat16* indX = nullptr;            // learned: feature rows [K][kp]
+    float *ind_seta = nullptr, *ind_y = nullptr;
+    double* ind_energy = nullptr;
+    unsigned char* ind_ok = nullptr;
+    int mlp_grid = 1;
     int* extent = nullptr;                    // arena: live extent {elements, faces} (null: all)
     unsigned long long* ind_stats = nullptr;  // [4] decision counts
     std::vector<double> Vinv_h;
@@ -188,6 +193,7 @@ class Engine {
         if (st_host) { cudaFreeHost(st_host); st_host = nullptr; }
         q = gRK = Qt = Qtmp = nullptr;
         mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr; nbr = nullptr; extent = nullptr;
+        indX = nullptr; ind_seta = ind_y = nullptr; ind_energy = nullptr; ind_ok = nullptr;
         indicator = 0;
         inited = copied = built = false;
     }
@@ -562,13 +568,24 @@ class Engine {
         ia.elem_inst = elem_inst; ia.st = st; ia.c = phys(); ia.stage0 = stage0;
         ia.P = mlpP; ia.Pb = mlpPb; ia.L = mlp_layout(NGL); ia.margin = ind_margin;
         ia.emin = ind_emin; ia.emax = ind_emax; ia.stats = ind_stats; ia.extent = extent;
+        ia.X = indX; ia.seta = ind_seta; ia.energy = ind_energy; ia.ok = ind_ok; ia.y = ind_y;
         using S = IndShape<NGL>;
         const int ntiles = (K + S::NE - 1) / S::NE;
-        if (indicator == 2)
-            k_indicator<NGL, true><<<std::min(ntiles, ind_grid[1]), S::THREADS, 0, stream>>>(ia, ntiles);
-        else
+        if (indicator == 2) {
+            if constexpr (NGL >= 4 && NGL <= 6) {
+                // the network as one batched GEMM over the elements:
+                // features, forward pass, then the sensor where unsure
+                constexpr int KP = mlp_kp(NGL);
+                k_ind_features<NGL><<<ntiles, S::THREADS, 0, stream>>>(ia);
+                k_mlp_forward<KP><<<mlp_grid, 128, MlpSmem<KP>::bytes(4), stream>>>(K, indX, mlpP, mlpPb, ind_y,
+                                                                                 ia.L, extent);
+                k_indicator<NGL, true><<<std::min(ntiles, ind_grid[1]), S::THREADS, 0, stream>>>(ia, ntiles);
+                launches += 3;
+            }
+        } else {
             k_indicator<NGL, false><<<std::min(ntiles, ind_grid[0]), S::THREADS, 0, stream>>>(ia, ntiles);
-        ++launches;
+            ++launches;
+        }
     }
 
     template <int NGL>
@@ -587,6 +604,16 @@ class Engine {
         if (e != cudaSuccess) return cuda_fail(e, "occupancy (indicator)");
         ind_grid[0] = std::max(1, o0) * sms;
         ind_grid[1] = std::max(1, o1) * sms;
+        if constexpr (NGL >= 4 && NGL <= 6) {
+            constexpr int KP = mlp_kp(NGL);
+            e = cudaFuncSetAttribute(k_mlp_forward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     MlpSmem<KP>::bytes(4));
+            int om = 0;
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&om, k_mlp_forward<KP>, 128, MlpSmem<KP>::bytes(4));
+            if (e != cudaSuccess) return cuda_fail(e, "occupancy (network)");
+            mlp_grid = std::max(1, std::min(std::max(1, om) * sms, (K + 63) / 64));
+        }
         return 0;
     }
 
@@ -626,7 +653,11 @@ class Engine {
         if (mode == 2) {
             const int n = mlp_layout(ngl).total;
             if (!mlpP) {
-                if ((r = alloc(&mlpP, (size_t)n)) || (r = alloc(&mlpPb, (size_t)n))) return r;
+                if ((r = alloc(&mlpP, (size_t)n)) || (r = alloc(&mlpPb, (size_t)n)) ||
+                    (r = alloc(&indX, (size_t)K * mlp_kp(ngl))) || (r = alloc(&ind_seta, (size_t)K)) ||
+                    (r = alloc(&ind_y, (size_t)K)) || (r = alloc(&ind_energy, (size_t)K)) ||
+                    (r = alloc(&ind_ok, (size_t)K)))
+                    return r;
                 cudaError_t e = cudaDeviceSynchronize();
                 if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
             }

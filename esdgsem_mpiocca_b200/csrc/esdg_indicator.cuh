@@ -52,6 +52,14 @@ struct IndArgs {
     // counts (optional): [0] zero by the net, [1] eps0 by the net,
     // [2] modal sensor, [3] elements with VP > 0
     unsigned long long* stats;
+    // learned: the network's inputs and outputs per element (k_ind_features
+    // and k_mlp_forward run first): feature rows X, s_eta, the nodal energy
+    // sum(eta^2), the positivity/finiteness check, the network output y
+    __nv_bfloat16* X;
+    float* seta;
+    double* energy;
+    unsigned char* ok;
+    float* y;
 };
 
 // Face neighbours of elements e0 .. e0+n-1 (-1 across walls): nbr[e] =
@@ -86,6 +94,115 @@ struct IndShape {
     static constexpr int ROWS = 16;  // feature rows per block (NE <= 16 for NGL >= 4)
 };
 
+
+// Learned pass 1: feature rows and the decision inputs of every live
+// element.  NE elements per block, one thread per node; the per-element
+// sums by shuffles where an element is an aligned group of lanes, else by
+// one thread per field over shared memory.
+template <int NGL>
+__global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs a) {
+    using S = IndShape<NGL>;
+    constexpr int N2 = S::N2, NE = S::NE, KP = mlp_kp(NGL);
+    constexpr bool GROUP = (32 % N2) == 0;
+    __shared__ double sv3[GROUP ? 1 : 3][GROUP ? 1 : NE * N2];
+    __shared__ double st_mean[GROUP ? 1 : NE][3], st_inv[GROUP ? 1 : NE][3];
+    const int tid = threadIdx.x;
+    const int el = tid / N2, nd = tid % N2;
+    const int e0 = blockIdx.x * NE;
+    if (a.extent && e0 >= a.extent[0]) return;  // whole block past the live extent
+    const int e = e0 + el;
+    const bool inb = e < a.K;
+    const bool live = inb && !a.st[inst_of(a.elem_inst, e)].done;
+    double v3[3] = {0.0, 0.0, 0.0}, h = 1.0;
+    if (inb) {
+        const long qid = (long)e * 3 * N2 + nd;
+        h = a.q[qid];
+        v3[0] = a.B[(long)e * N2 + nd] + h;
+        v3[1] = a.q[qid + N2];
+        v3[2] = a.q[qid + 2 * N2];
+    }
+    __nv_bfloat16* xr = a.X + (long)e * KP;
+    double mh = h, e2 = v3[0] * v3[0];
+    bool fin = isfinite(h) && isfinite(v3[1]) && isfinite(v3[2]);
+    if constexpr (GROUP) {
+#pragma unroll
+        for (int off = N2 / 2; off > 0; off >>= 1) {
+            mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
+            e2 += __shfl_xor_sync(0xffffffffu, e2, off);
+            fin = __shfl_xor_sync(0xffffffffu, (int)fin, off) && fin;
+        }
+        // the three fields' reductions interleaved (independent chains)
+        double m3[3] = {v3[0], v3[1], v3[2]}, d3[3];
+#pragma unroll
+        for (int off = N2 / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int f = 0; f < 3; ++f) m3[f] += __shfl_xor_sync(0xffffffffu, m3[f], off);
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            m3[f] /= N2;
+            d3[f] = (v3[f] - m3[f]) * (v3[f] - m3[f]);
+        }
+#pragma unroll
+        for (int off = N2 / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int f = 0; f < 3; ++f) d3[f] += __shfl_xor_sync(0xffffffffu, d3[f], off);
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            const double m = m3[f], d2 = d3[f];
+            const double rms = sqrt(d2 / N2);
+            const double inv = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
+            if (live) {
+                xr[f * N2 + nd] = __float2bfloat16((float)((v3[f] - m) * inv));
+                if (nd == f) {
+                    const double tot = m * m + rms * rms;
+                    const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
+                    xr[3 * N2 + f] = __float2bfloat16((float)(0.25 * sf));
+                    if (f == 0) a.seta[e] = (float)sf;
+                }
+            }
+        }
+    } else {
+        for (int f = 0; f < 3; ++f) sv3[f][tid] = v3[f];
+        __syncthreads();
+        if (nd < 3) {
+            const double* v = &sv3[nd][el * N2];
+            double m = 0.0;
+            for (int p = 0; p < N2; ++p) m += v[p];
+            m /= N2;
+            double d2 = 0.0;
+            for (int p = 0; p < N2; ++p) d2 += (v[p] - m) * (v[p] - m);
+            const double rms = sqrt(d2 / N2);
+            st_mean[el][nd] = m;
+            st_inv[el][nd] = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
+            const double tot = m * m + rms * rms;
+            const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
+            if (live) {
+                xr[3 * N2 + nd] = __float2bfloat16((float)(0.25 * sf));
+                if (nd == 0) a.seta[e] = (float)sf;
+            }
+        } else if (nd == 3) {
+            for (int p = 0; p < N2; ++p) {
+                const double hp = a.q[(long)e * 3 * N2 + p];  // L1-resident: this block just read it
+                mh = fmin(mh, hp);
+                fin = fin && isfinite(hp) && isfinite(sv3[1][el * N2 + p]) && isfinite(sv3[2][el * N2 + p]);
+            }
+            e2 = 0.0;
+            for (int p = 0; p < N2; ++p) e2 += sv3[0][el * N2 + p] * sv3[0][el * N2 + p];
+        }
+        __syncthreads();
+        if (live)
+            for (int f = 0; f < 3; ++f)
+                xr[f * N2 + nd] = __float2bfloat16((float)((v3[f] - st_mean[el][f]) * st_inv[el][f]));
+    }
+    if (live) {
+        for (int c = 3 * N2 + 3 + nd; c < KP; c += N2) xr[c] = __float2bfloat16(0.0f);
+        if (nd == (GROUP ? 0 : 3)) {
+            a.energy[e] = e2;
+            a.ok[e] = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
+        }
+    }
+}
+
 // The learned decision for one element: 1 when the modal sensor must decide.
 __device__ __forceinline__ int learned_needs_modal(const IndArgs& a, double sig, double nodal, int ok) {
     if (!ok) return 1;                                // positivity / finiteness check failed
@@ -98,72 +215,54 @@ __device__ __forceinline__ int learned_needs_modal(const IndArgs& a, double sig,
 
 // One node's inputs, loaded a tile ahead.
 struct IndLoad {
-    double h, b, hu, hv;
+    double h, b;
     int ins;
     int4 nb;
 };
 
-template <int NGL, bool LEARNED>
+template <int NGL>
 __device__ __forceinline__ IndLoad ind_load(const IndArgs& a, int t) {
     using S = IndShape<NGL>;
     constexpr int N2 = S::N2;
     const int el = threadIdx.x / N2, nd = threadIdx.x % N2;
     const int e = t * S::NE + el;
-    IndLoad L{0.0, 0.0, 0.0, 0.0, -1, make_int4(-1, -1, -1, -1)};
+    IndLoad L{0.0, 0.0, -1, make_int4(-1, -1, -1, -1)};
     if (e < a.K) {
-        const long qid = (long)e * 3 * N2 + nd;
-        L.h = a.q[qid];
+        L.h = a.q[(long)e * 3 * N2 + nd];
         L.b = a.B[(long)e * N2 + nd];
-        if (LEARNED) {
-            L.hu = a.q[qid + N2];
-            L.hv = a.q[qid + 2 * N2];
-        }
         L.ins = inst_of(a.elem_inst, e);
         if (nd == 0) L.nb = a.nbr[e];
     }
     return L;
 }
 
-// Persistent: each block walks tiles of NE elements, the next tile's loads
-// in flight while the current one is processed.
+// The sensor pass (the learned variant after k_ind_features and
+// k_mlp_forward).  Persistent: each block walks tiles of NE elements, the
+// next tiles' loads in flight while the current one is processed.
 template <int NGL, bool LEARNED>
 __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs a, int ntiles) {
     using S = IndShape<NGL>;
-    constexpr int N2 = S::N2, NE = S::NE, KP = S::KP;
-    if constexpr (LEARNED && NE > S::ROWS) {
-        return;  // more elements per block than one MMA tile: never launched (N >= 3 only)
-    }
-    constexpr int NEL = LEARNED ? NE : 1;  // sized for the learned path only
+    constexpr int N2 = S::N2, NE = S::NE;
     if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     // an element's nodes form an aligned group of lanes (N2 divides 32)
     constexpr bool GROUP = (32 % N2) == 0;
     __shared__ double sV[N2];
     __shared__ double seta[NE * N2], sM[NE * N2], sW[NE * N2];
-    __shared__ double sh[NEL * N2], su[NEL * N2], sv[NEL * N2];
-    __shared__ double fmean[NEL][3], finv[NEL][3];
-    __shared__ double fs_eta[NEL], fE[NEL];
-    __shared__ int fok[NEL];
     __shared__ int need[NE];
-    __shared__ __align__(32) __nv_bfloat16 sX[LEARNED ? S::ROWS * KP : 16];
-    __shared__ __align__(32) __nv_bfloat16 sW1[LEARNED ? MLP_H * KP : 16];
-    __shared__ __align__(32) __nv_bfloat16 sW2[LEARNED ? MLP_H * MLP_H : 16];
-    __shared__ float y16[16];
+    __shared__ int verdict[NE];  // learned: 0 zero, 1 eps0 (when need == 0)
 
     const int tid = threadIdx.x;
     const int el = tid / N2, nd = tid % N2;
     const int s = el * N2 + nd;
     if (tid < N2) sV[tid] = a.Vinv[tid];
-    if (LEARNED) mlp_stage_weights(KP, a.Pb, a.L, sW1, sW2);
     unsigned long long cnt[4] = {0, 0, 0, 0};
-    // loads run PF tiles ahead: enough bytes in flight per SM to cover the
-    // memory latency at a few blocks per SM
-    constexpr int PF = LEARNED ? 1 : 2;
+    constexpr int PF = 2;  // tiles of loads in flight
     int t = blockIdx.x;
     IndLoad ring[PF];
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
         const int tk = t + k * gridDim.x;
-        ring[k] = (tk < ntiles) ? ind_load<NGL, LEARNED>(a, tk) : IndLoad{};
+        ring[k] = (tk < ntiles) ? ind_load<NGL>(a, tk) : IndLoad{};
     }
     for (; t < ntiles; t += gridDim.x) {
         const IndLoad cur = ring[0];
@@ -171,139 +270,37 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
         for (int k = 0; k + 1 < PF; ++k) ring[k] = ring[k + 1];
         {
             const int tn = t + PF * gridDim.x;
-            ring[PF - 1] = (tn < ntiles) ? ind_load<NGL, LEARNED>(a, tn) : IndLoad{};
+            ring[PF - 1] = (tn < ntiles) ? ind_load<NGL>(a, tn) : IndLoad{};
         }
         const int e = t * NE + el;
         const bool live = e < a.K && !a.st[cur.ins].done;
         seta[s] = cur.b + cur.h;
-        if (LEARNED) {
-            sh[s] = cur.h;
-            su[s] = cur.hu;
-            sv[s] = cur.hv;
+        if (nd == 0) {
+            int nm = 1, vd = 0;
+            if (LEARNED && live) {
+                const double sig = (double)a.y[e] + (double)a.seta[e];
+                const double nodal = a.energy[e];
+                nm = learned_needs_modal(a, sig, nodal, a.ok[e]);
+                vd = (nm == 0 && a.emax * nodal >= a.c.ZeroTOL && sig > a.c.sigmaMax + a.margin) ? 1 : 0;
+            }
+            need[el] = nm;
+            verdict[el] = vd;
         }
-        if (nd == 0) need[el] = LEARNED ? 0 : 1;
-        __syncthreads();
-
-        if (LEARNED && GROUP) {
-            // an element is a group of N2 lanes: statistics by shuffles
-            const double v3[3] = {cur.b + cur.h, cur.hu, cur.hv};
-            double mh = cur.h;
-            bool fin = isfinite(cur.h) && isfinite(cur.hu) && isfinite(cur.hv);
-#pragma unroll
-            for (int off = N2 / 2; off > 0; off >>= 1) {
-                mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
-                fin = __shfl_xor_sync(0xffffffffu, (int)fin, off) && fin;
-            }
-#pragma unroll
-            for (int f = 0; f < 3; ++f) {
-                double m = v3[f];
-#pragma unroll
-                for (int off = N2 / 2; off > 0; off >>= 1) m += __shfl_xor_sync(0xffffffffu, m, off);
-                m /= N2;
-                double d2 = (v3[f] - m) * (v3[f] - m);
-#pragma unroll
-                for (int off = N2 / 2; off > 0; off >>= 1) d2 += __shfl_xor_sync(0xffffffffu, d2, off);
-                const double rms = sqrt(d2 / N2);
-                const double tot = m * m + rms * rms;
-                const double inv = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
-                sX[el * KP + f * N2 + nd] = __float2bfloat16((float)((v3[f] - m) * inv));
-                if (nd == f) {
-                    const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
-                    sX[el * KP + 3 * N2 + f] = __float2bfloat16((float)(0.25 * sf));
-                    if (f == 0) {
-                        fs_eta[el] = sf;
-                        fE[el] = tot;
-                    }
-                }
-            }
-            if (nd == 0) fok[el] = fin && mh > a.c.PosPresTOL;
-            for (int i = tid; i < S::ROWS * KP; i += S::THREADS) {
-                const int r = i / KP, c = i % KP;
-                if (r >= NE || t * NE + r >= a.K || c >= 3 * N2 + 3) sX[i] = __float2bfloat16(0.0f);
-            }
-            __syncthreads();
-            if (tid < 32) {
-                float ylo, yhi;
-                mlp_warp_forward_regs<KP>(sX, sW1, sW2, a.P, a.L, ylo, yhi);
-                if ((tid & 3) == 0) {
-                    y16[tid >> 2] = ylo;
-                    y16[(tid >> 2) + 8] = yhi;
-                }
-            }
-            __syncthreads();
-            if (live && nd == 0) need[el] = learned_needs_modal(a, (double)y16[el] + fs_eta[el], fE[el] * N2, fok[el]);
-        } else if (LEARNED) {
-            // per-element statistics: threads nd = 0, 1, 2 take a field each,
-            // nd = 3 the positivity and finiteness check
-            if (live && nd < 3) {
-                const double* v = (nd == 0) ? seta + el * N2 : (nd == 1 ? su + el * N2 : sv + el * N2);
-                double m = 0.0;
-                for (int p = 0; p < N2; ++p) m += v[p];
-                m /= N2;
-                double d2 = 0.0;
-                for (int p = 0; p < N2; ++p) d2 += (v[p] - m) * (v[p] - m);
-                const double rms = sqrt(d2 / N2);
-                const double tot = m * m + rms * rms;
-                const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
-                fmean[el][nd] = m;
-                finv[el][nd] = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
-                sX[el * KP + 3 * N2 + nd] = __float2bfloat16((float)(0.25 * sf));
-                if (nd == 0) {
-                    fs_eta[el] = sf;
-                    fE[el] = tot;
-                }
-            } else if (live && nd == 3) {
-                double mh = 1e300;
-                bool fin = true;
-                for (int p = 0; p < N2; ++p) {
-                    const double h = sh[el * N2 + p];
-                    mh = fmin(mh, h);
-                    fin = fin && isfinite(h) && isfinite(su[el * N2 + p]) && isfinite(sv[el * N2 + p]);
-                }
-                fok[el] = fin && mh > a.c.PosPresTOL;
-            }
-            // zero rows of absent elements, and the padding columns
-            for (int i = tid; i < S::ROWS * KP; i += S::THREADS) {
-                const int r = i / KP, c = i % KP;
-                if (r >= NE || t * NE + r >= a.K || c >= 3 * N2 + 3) sX[i] = __float2bfloat16(0.0f);
-            }
-            __syncthreads();
-            if (live) {
-#pragma unroll
-                for (int f = 0; f < 3; ++f) {
-                    const double v = (f == 0) ? seta[s] : (f == 1 ? su[s] : sv[s]);
-                    sX[el * KP + f * N2 + nd] = __float2bfloat16((float)((v - fmean[el][f]) * finv[el][f]));
-                }
-            }
-            __syncthreads();
-            if (tid < 32) {
-                float ylo, yhi;
-                mlp_warp_forward_regs<KP>(sX, sW1, sW2, a.P, a.L, ylo, yhi);
-                if ((tid & 3) == 0) {
-                    y16[tid >> 2] = ylo;
-                    y16[(tid >> 2) + 8] = yhi;
-                }
-            }
-            __syncthreads();
-            if (live && nd == 0) need[el] = learned_needs_modal(a, (double)y16[el] + fs_eta[el], fE[el] * N2, fok[el]);
-        }
-        // modal sensor where needed (every element without the network)
-        const bool any = LEARNED ? __syncthreads_or(live && nd == 0 && need[el]) : true;
+        // the modal transform where the sensor decides (every element
+        // without the network)
+        const bool any = LEARNED ? __syncthreads_or(live && nd == 0 && need[el]) : (__syncthreads(), true);
+        bool clear = false;
         if (any) {
             const int i = nd / NGL, j = nd % NGL;  // entry (i, j) of M1 and w
             sM[s] = sensor_m1<NGL>(sV, seta + el * N2, i, j);
             __syncthreads();
             sW[s] = sensor_w<NGL>(sV, sM + el * N2, i, j);
             __syncthreads();
-        }
-        // Screen: the energy ratios from sums in any order (shuffles) differ
-        // from the reference-order ones by rounding only; far below the
-        // 10^sigma_min bound the sensor is exactly zero, so the serial
-        // reference-order tail runs only where it can give something else.
-        bool clear = false;
-        if constexpr (GROUP) {
-            if (any) {
-                const int i = nd / NGL, j = nd % NGL;
+            // Screen: energy ratios from sums in any order (shuffles) differ
+            // from the reference-order ones by rounding only; far below the
+            // 10^sigma_min bound the sensor is exactly zero, so the serial
+            // reference-order tail runs only where it can give otherwise.
+            if constexpr (GROUP) {
                 const double w = sW[s], w2 = w * w;
                 constexpr int N = NGL - 1;
                 double z1 = ((i == N) || (j == N)) ? w2 : 0.0;
@@ -325,14 +322,12 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
         }
         if (live && nd == 0) {
             double v = 0.0;
-            int kind = 0;  // 0 net zero, 1 net eps0, 2 modal
+            int kind = 2;  // 0 net zero, 1 net eps0, 2 modal
             if (need[el]) {
                 v = clear ? 0.0 : sensor_tail<NGL>(a.c, sW + el * N2);
-                kind = 2;
-            } else if (LEARNED) {
-                const double sig = (double)y16[el] + fs_eta[el];
-                const double nodal = fE[el] * (double)N2;
-                if (a.emax * nodal >= a.c.ZeroTOL && sig > a.c.sigmaMax + a.margin) { v = a.c.eps0; kind = 1; }
+            } else {
+                kind = verdict[el];
+                v = kind ? a.c.eps0 : 0.0;
             }
             a.VP[e] = v;
             if (a.stage0 && v > 0.0) atomicMax(&a.st[cur.ins].visc_key, dbl_key(v));
@@ -342,7 +337,7 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
         }
         __syncthreads();  // shared tiles are rewritten next iteration
     }
-    if (a.stats && nd == 0) {
+    if (a.stats) {
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (cnt[k]) atomicAdd(&a.stats[k], cnt[k]);

@@ -367,7 +367,8 @@ template <int KP>
 __global__ void __launch_bounds__(128) k_mlp_forward(int M, const __nv_bfloat16* __restrict__ X,
                                                      const float* __restrict__ P,
                                                      const __nv_bfloat16* __restrict__ Pb, float* __restrict__ y,
-                                                     MlpLayout L) {
+                                                     MlpLayout L, const int* __restrict__ Mlive = nullptr) {
+    if (Mlive) M = min(M, *Mlive);  // rows past a live extent are skipped
     using S = MlpSmem<KP>;
     extern __shared__ __align__(128) unsigned char mlp_smem[];
     __nv_bfloat16* sW1 = reinterpret_cast<__nv_bfloat16*>(mlp_smem);
