@@ -197,11 +197,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="curved_lake", choices=["curved_lake", "ensemble", "serving"],
+    ap.add_argument("--workload", default="curved_lake", choices=["curved_lake", "ensemble", "serving", "dambreak"],
                     help="curved_lake: the headline single-mesh workload; ensemble: 256 seeded tsunami "
-                         "members batched vs one at a time; serving: Poisson request streams")
+                         "members batched vs one at a time; serving: Poisson request streams; dambreak: the "
+                         "learned indicator against the plain sensor on the N=4 dam break")
     ap.add_argument("--rates", default="10,100,1000", help="serving workload: arrival rates (requests/s)")
-    ap.add_argument("--requests", type=int, default=24, help="serving workload: requests per rate")
+    ap.add_argument("--requests", type=int, default=48, help="serving workload: requests per rate")
     ap.add_argument("--hbm-gb", type=float, default=40.0, help="serving workload: HBM given to the arenas")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--alone-members", type=int, default=15,
@@ -211,6 +212,8 @@ def main():
         return ensemble_bench(args)
     if args.workload == "serving":
         return serving_bench(args)
+    if args.workload == "dambreak":
+        return dambreak_bench(args)
     ws, rank, local = dist_env()
     args.warmup = max(args.warmup, 3)
 
@@ -512,7 +515,12 @@ def serving_bench(args):
             out.append({"rate_per_s": rate, "batched": b, "plain_one_at_a_time": a,
                         "throughput_ratio": b["throughput_dof_stages_per_s"] / a["throughput_dof_stages_per_s"],
                         "p99_ratio": a["p99_s"] / b["p99_s"]})
-    srv.close()
+        srv.close()
+        # the same server architecture with the exact modal active set
+        srv1 = serving.Server(hbm_bytes=args.hbm_gb * 1e9, max_instances=256, device_id=local, indicator=1)
+        serving.serve(serving.make_requests(2, 1e6, seed=7, sizes=(32,), horizons=(5, 5)), srv1, realtime=False)
+        m1 = serving.serve(serving.fresh(streams[rates[-1]]), srv1, realtime=True)
+        srv1.close()
     top = out[-1]["batched"]
     line = {"metric": METRIC, "value": top["throughput_dof_stages_per_s"] * ws, "unit": UNIT, "n_gpus": ws,
             "steps": None, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
@@ -522,7 +530,79 @@ def serving_bench(args):
                                    "200-2000 steps, continuous batching with admission by HBM footprint "
                                    f"({args.hbm_gb} GB of arenas), learned indicator + active set",
                        "setup_s": setup_s, "value_is": f"batched throughput at {rates[-1]} requests/s"},
-            "rates": out, "clocks": ck.result}
+            "rates": out, "batched_modal_active_set_at_top_rate": m1, "clocks": ck.result}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def dambreak_bench(args):
+    """The learned-indicator configuration: circular dam break, N=4 on 256^2
+    curved quads, flat bottom, artificial viscosity, 2000 steps; the plain
+    path (modal sensor, viscous terms everywhere), the exact modal active set
+    and the learned indicator from the same initial state.  Reports their
+    rates, the learned run's deviation from the plain run (relative L2 per
+    variable) and the flag agreement of the two indicators on the plain
+    run's states."""
+    import torch
+    from esdgsem_mpiocca_b200 import problems
+    from esdgsem_mpiocca_b200.deviceclass import Solver
+    from esdgsem_mpiocca_b200.indicator import IndicatorNet
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    steps = args.steps if args.steps != 400 else 2000
+    warm = max(args.warmup, 3)
+    prob = problems.dam_break(N=4, nel=256, seed=rank, steps=steps + warm)
+    net = IndicatorNet.default(4)
+    stream = torch.cuda.Stream()
+    runs = {}
+    with Clocks(local) as ck:
+        for mode in (0, 1, 2):
+            s = Solver(prob, device_id=local, indicator=mode, net=net if mode == 2 else None)
+            s.dc.set_stream(stream.cuda_stream)
+            s.run(T=1e9, max_steps=warm)
+            if mode:
+                s.dc.indicator_stats(reset=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                s.dc.advance(steps, 1e9)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            runs[mode] = {"ms": ms, "rate": prob.dofs() * STAGES * steps / (ms / 1e3), "q": s.q(),
+                          "stats": s.dc.indicator_stats() if mode else None}
+            s.close()
+    K, n2 = prob.K, prob.ngl ** 2
+    q0 = runs[0]["q"].reshape(K, 3, n2)
+    dev = {}
+    for mode in (1, 2):
+        qm = runs[mode]["q"].reshape(K, 3, n2)
+        dev[mode] = [float(np.linalg.norm(qm[:, v] - q0[:, v]) / np.linalg.norm(q0[:, v])) for v in range(3)]
+    # flag agreement on the plain run's final state
+    s0 = Solver(prob, device_id=local, q0=runs[0]["q"])
+    _, v0 = s0.rhs()
+    s0.close()
+    s2 = Solver(prob, device_id=local, q0=runs[0]["q"], indicator=2, net=net)
+    _, v2 = s2.rhs()
+    s2.close()
+    st = runs[2]["stats"]
+    ev = st["net_zero"] + st["net_full"] + st["modal"]
+    line = {"metric": METRIC, "value": runs[2]["rate"], "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warm,
+            "ms_per_step": runs[2]["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (indicator network: bf16 weights, fp32 accumulation)",
+            "data": "synthetic (seeded circular dam break)",
+            "config": {"workload": f"dam break: N=4, 256x256 curved quads, b=0, artificial viscosity, {steps} steps; "
+                                   "learned indicator + active set", "nodes": prob.dofs(),
+                       "radius": prob.meta["radius"]},
+            "plain_modal_full_path": runs[0]["rate"], "modal_active_set": runs[1]["rate"],
+            "ratio_learned_over_plain": runs[2]["rate"] / runs[0]["rate"],
+            "rel_l2_deviation_learned_vs_plain": dev[2], "rel_l2_deviation_active_set_vs_plain": dev[1],
+            "flag_agreement_final_state": float(((v0 > 0) == (v2 > 0)).mean()),
+            "viscosity_identical_final_state": float((v0 == v2).mean()),
+            "network_settled": (st["net_zero"] + st["net_full"]) / max(ev, 1),
+            "viscous_share": st["viscous"] / max(ev, 1), "clocks": ck.result}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

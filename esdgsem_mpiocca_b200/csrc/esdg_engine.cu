@@ -576,7 +576,10 @@ class Engine {
                 // the network as one batched GEMM over the elements:
                 // features, forward pass, then the sensor where unsure
                 constexpr int KP = mlp_kp(NGL);
-                k_ind_features<NGL><<<ntiles, S::THREADS, 0, stream>>>(ia);
+                if constexpr ((32 % (NGL * NGL)) == 0)
+                    k_ind_features<NGL><<<ntiles, S::THREADS, 0, stream>>>(ia);
+                else
+                    k_ind_features_warp<NGL><<<(K + 7) / 8, 256, 0, stream>>>(ia);
                 k_mlp_forward<KP><<<mlp_grid, 128, MlpSmem<KP>::bytes(4), stream>>>(K, indX, mlpP, mlpPb, ind_y,
                                                                                  ia.L, extent);
                 k_indicator<NGL, true><<<std::min(ntiles, ind_grid[1]), S::THREADS, 0, stream>>>(ia, ntiles);

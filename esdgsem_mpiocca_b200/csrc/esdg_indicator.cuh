@@ -203,6 +203,80 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs
     }
 }
 
+// Learned pass 1 for degrees whose element is not an aligned lane group
+// (n^2 does not divide 32): one warp per element (nodes lane, lane + 32,
+// ...), the three fields' sums interleaved, no block-wide barrier.
+template <int NGL>
+__global__ void __launch_bounds__(256) k_ind_features_warp(IndArgs a) {
+    constexpr int N2 = NGL * NGL, R = (N2 + 31) / 32, KP = mlp_kp(NGL);
+    const int lane = threadIdx.x & 31;
+    const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (e >= a.K || (a.extent && e >= a.extent[0])) return;  // warp-uniform
+    if (a.st[inst_of(a.elem_inst, e)].done) return;
+    const double* qe = a.q + (long)e * 3 * N2;
+    double v[3][R];
+    double mh = 1e300, e2 = 0.0, m3[3] = {0.0, 0.0, 0.0};
+    bool fin = true;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int p = lane + 32 * k;
+        v[0][k] = v[1][k] = v[2][k] = 0.0;
+        if (p < N2) {
+            const double h = qe[p];
+            v[0][k] = a.B[(long)e * N2 + p] + h;
+            v[1][k] = qe[p + N2];
+            v[2][k] = qe[p + 2 * N2];
+            mh = fmin(mh, h);
+            fin = fin && isfinite(h) && isfinite(v[1][k]) && isfinite(v[2][k]);
+            e2 += v[0][k] * v[0][k];
+#pragma unroll
+            for (int f = 0; f < 3; ++f) m3[f] += v[f][k];
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int f = 0; f < 3; ++f) m3[f] += __shfl_xor_sync(0xffffffffu, m3[f], off);
+        mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
+        e2 += __shfl_xor_sync(0xffffffffu, e2, off);
+    }
+    fin = __all_sync(0xffffffffu, fin);
+    double d3[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        m3[f] /= N2;
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+            if (lane + 32 * k < N2) d3[f] += (v[f][k] - m3[f]) * (v[f][k] - m3[f]);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int f = 0; f < 3; ++f) d3[f] += __shfl_xor_sync(0xffffffffu, d3[f], off);
+    __nv_bfloat16* xr = a.X + (long)e * KP;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        const double m = m3[f], rms = sqrt(d3[f] / N2);
+        const double inv = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int p = lane + 32 * k;
+            if (p < N2) xr[f * N2 + p] = __float2bfloat16((float)((v[f][k] - m) * inv));
+        }
+        if (lane == f) {
+            const double tot = m * m + rms * rms;
+            const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
+            xr[3 * N2 + f] = __float2bfloat16((float)(0.25 * sf));
+            if (f == 0) a.seta[e] = (float)sf;
+        }
+    }
+    for (int c = 3 * N2 + 3 + lane; c < KP; c += 32) xr[c] = __float2bfloat16(0.0f);
+    if (lane == 0) {
+        a.energy[e] = e2;
+        a.ok[e] = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
+    }
+}
+
 // The learned decision for one element: 1 when the modal sensor must decide.
 __device__ __forceinline__ int learned_needs_modal(const IndArgs& a, double sig, double nodal, int ok) {
     if (!ok) return 1;                                // positivity / finiteness check failed
