@@ -577,10 +577,10 @@ class Engine {
                 // features, forward pass, then the sensor where unsure
                 constexpr int KP = mlp_kp(NGL);
                 if constexpr ((32 % (NGL * NGL)) == 0)
-                    k_ind_features<NGL><<<ntiles, S::THREADS, 0, stream>>>(ia);
+                    k_ind_features<NGL><<<std::min(ntiles, ind_grid[0]), S::THREADS, 0, stream>>>(ia, ntiles);
                 else
                     k_ind_features_warp<NGL><<<(K + 7) / 8, 256, 0, stream>>>(ia);
-                k_mlp_forward<KP><<<mlp_grid, 128, MlpSmem<KP>::bytes(4), stream>>>(K, indX, mlpP, mlpPb, ind_y,
+                k_mlp_forward<KP><<<mlp_grid, 128, MlpSmem<KP>::fwd_bytes(4), stream>>>(K, indX, mlpP, mlpPb, ind_y,
                                                                                  ia.L, extent);
                 k_indicator<NGL, true><<<std::min(ntiles, ind_grid[1]), S::THREADS, 0, stream>>>(ia, ntiles);
                 launches += 3;
@@ -610,10 +610,11 @@ class Engine {
         if constexpr (NGL >= 4 && NGL <= 6) {
             constexpr int KP = mlp_kp(NGL);
             e = cudaFuncSetAttribute(k_mlp_forward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     MlpSmem<KP>::bytes(4));
+                                     MlpSmem<KP>::fwd_bytes(4));
             int om = 0;
             if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&om, k_mlp_forward<KP>, 128, MlpSmem<KP>::bytes(4));
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&om, k_mlp_forward<KP>, 128,
+                                                                  MlpSmem<KP>::fwd_bytes(4));
             if (e != cudaSuccess) return cuda_fail(e, "occupancy (network)");
             mlp_grid = std::max(1, std::min(std::max(1, om) * sms, (K + 63) / 64));
         }

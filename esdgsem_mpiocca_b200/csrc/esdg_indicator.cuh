@@ -96,107 +96,88 @@ struct IndShape {
 
 
 // Learned pass 1: feature rows and the decision inputs of every live
-// element.  NE elements per block, one thread per node; the per-element
-// sums by shuffles where an element is an aligned group of lanes, else by
-// one thread per field over shared memory.
+// element, for degrees whose element is an aligned group of lanes (n^2
+// divides 32): NE elements per tile, one thread per node, the per-element
+// sums by shuffles within the group, no block-wide barrier.  Persistent,
+// the next tile's loads in flight while a tile is processed.
 template <int NGL>
-__global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs a) {
+__global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs a, int ntiles) {
     using S = IndShape<NGL>;
     constexpr int N2 = S::N2, NE = S::NE, KP = mlp_kp(NGL);
-    constexpr bool GROUP = (32 % N2) == 0;
-    __shared__ double sv3[GROUP ? 1 : 3][GROUP ? 1 : NE * N2];
-    __shared__ double st_mean[GROUP ? 1 : NE][3], st_inv[GROUP ? 1 : NE][3];
+    static_assert((32 % N2) == 0, "element = aligned lane group");
+    if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     const int tid = threadIdx.x;
     const int el = tid / N2, nd = tid % N2;
-    const int e0 = blockIdx.x * NE;
-    if (a.extent && e0 >= a.extent[0]) return;  // whole block past the live extent
-    const int e = e0 + el;
-    const bool inb = e < a.K;
-    const bool live = inb && !a.st[inst_of(a.elem_inst, e)].done;
-    double v3[3] = {0.0, 0.0, 0.0}, h = 1.0;
-    if (inb) {
-        const long qid = (long)e * 3 * N2 + nd;
-        h = a.q[qid];
-        v3[0] = a.B[(long)e * N2 + nd] + h;
-        v3[1] = a.q[qid + N2];
-        v3[2] = a.q[qid + 2 * N2];
-    }
-    __nv_bfloat16* xr = a.X + (long)e * KP;
-    double mh = h, e2 = v3[0] * v3[0];
-    bool fin = isfinite(h) && isfinite(v3[1]) && isfinite(v3[2]);
-    if constexpr (GROUP) {
+    struct Ld {
+        double h, b, hu, hv;
+        int ins;
+    };
+    auto fetch = [&](int t) {
+        Ld L{1.0, 0.0, 0.0, 0.0, -1};
+        const int e = t * NE + el;
+        if (e < a.K) {
+            const long qid = (long)e * 3 * N2 + nd;
+            L.h = a.q[qid];
+            L.b = a.B[(long)e * N2 + nd];
+            L.hu = a.q[qid + N2];
+            L.hv = a.q[qid + 2 * N2];
+            L.ins = inst_of(a.elem_inst, e);
+        }
+        return L;
+    };
+    int t = blockIdx.x;
+    Ld nxt = (t < ntiles) ? fetch(t) : Ld{1.0, 0.0, 0.0, 0.0, -1};
+    for (; t < ntiles; t += gridDim.x) {
+        const Ld cur = nxt;
+        if (t + gridDim.x < ntiles) nxt = fetch(t + gridDim.x);
+        const int e = t * NE + el;
+        const bool live = e < a.K && !a.st[cur.ins].done;
+        const double v3[3] = {cur.b + cur.h, cur.hu, cur.hv};
+        double mh = cur.h, e2 = v3[0] * v3[0];
+        bool fin = isfinite(cur.h) && isfinite(cur.hu) && isfinite(cur.hv);
+        double m3[3] = {v3[0], v3[1], v3[2]}, d3[3];
 #pragma unroll
         for (int off = N2 / 2; off > 0; off >>= 1) {
+#pragma unroll
+            for (int f = 0; f < 3; ++f) m3[f] += __shfl_xor_sync(0xffffffffu, m3[f], off);
             mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
             e2 += __shfl_xor_sync(0xffffffffu, e2, off);
             fin = __shfl_xor_sync(0xffffffffu, (int)fin, off) && fin;
         }
-        // the three fields' reductions interleaved (independent chains)
-        double m3[3] = {v3[0], v3[1], v3[2]}, d3[3];
-#pragma unroll
-        for (int off = N2 / 2; off > 0; off >>= 1)
-#pragma unroll
-            for (int f = 0; f < 3; ++f) m3[f] += __shfl_xor_sync(0xffffffffu, m3[f], off);
+        // deviations from the (double) mean; their statistics in single
+        // precision, which is all the BF16 features need
+        float dv[3], d3f[3];
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
             m3[f] /= N2;
-            d3[f] = (v3[f] - m3[f]) * (v3[f] - m3[f]);
+            dv[f] = (float)(v3[f] - m3[f]);
+            d3f[f] = dv[f] * dv[f];
         }
 #pragma unroll
         for (int off = N2 / 2; off > 0; off >>= 1)
 #pragma unroll
-            for (int f = 0; f < 3; ++f) d3[f] += __shfl_xor_sync(0xffffffffu, d3[f], off);
+            for (int f = 0; f < 3; ++f) d3f[f] += __shfl_xor_sync(0xffffffffu, d3f[f], off);
+        (void)d3;
+        if (!live) continue;  // after the shuffles: the whole group skips together
+        __nv_bfloat16* xr = a.X + (long)e * KP;
+        float rmsf[3];
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
-            const double m = m3[f], d2 = d3[f];
-            const double rms = sqrt(d2 / N2);
-            const double inv = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
-            if (live) {
-                xr[f * N2 + nd] = __float2bfloat16((float)((v3[f] - m) * inv));
-                if (nd == f) {
-                    const double tot = m * m + rms * rms;
-                    const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
-                    xr[3 * N2 + f] = __float2bfloat16((float)(0.25 * sf));
-                    if (f == 0) a.seta[e] = (float)sf;
-                }
-            }
+            rmsf[f] = sqrtf(d3f[f] * (1.0f / N2));
+            const float mf = fabsf((float)m3[f]);
+            const float inv = (rmsf[f] > (float)MLP_REL_FLAT * mf && rmsf[f] > 0.0f) ? 1.0f / rmsf[f] : 0.0f;
+            xr[f * N2 + nd] = __float2bfloat16(dv[f] * inv);
         }
-    } else {
-        for (int f = 0; f < 3; ++f) sv3[f][tid] = v3[f];
-        __syncthreads();
-        if (nd < 3) {
-            const double* v = &sv3[nd][el * N2];
-            double m = 0.0;
-            for (int p = 0; p < N2; ++p) m += v[p];
-            m /= N2;
-            double d2 = 0.0;
-            for (int p = 0; p < N2; ++p) d2 += (v[p] - m) * (v[p] - m);
-            const double rms = sqrt(d2 / N2);
-            st_mean[el][nd] = m;
-            st_inv[el][nd] = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
-            const double tot = m * m + rms * rms;
-            const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
-            if (live) {
-                xr[3 * N2 + nd] = __float2bfloat16((float)(0.25 * sf));
-                if (nd == 0) a.seta[e] = (float)sf;
-            }
-        } else if (nd == 3) {
-            for (int p = 0; p < N2; ++p) {
-                const double hp = a.q[(long)e * 3 * N2 + p];  // L1-resident: this block just read it
-                mh = fmin(mh, hp);
-                fin = fin && isfinite(hp) && isfinite(sv3[1][el * N2 + p]) && isfinite(sv3[2][el * N2 + p]);
-            }
-            e2 = 0.0;
-            for (int p = 0; p < N2; ++p) e2 += sv3[0][el * N2 + p] * sv3[0][el * N2 + p];
+        if (nd < 3) {  // lanes 0, 1, 2 of the group: the scale feature of their field, one log10 pass
+            const float r = nd == 0 ? rmsf[0] : (nd == 1 ? rmsf[1] : rmsf[2]);
+            const float m = (float)(nd == 0 ? m3[0] : (nd == 1 ? m3[1] : m3[2]));
+            const float tot = m * m + r * r;
+            const float sf = (tot > 0.0f && r > 0.0f) ? fmaxf(log10f(r * r / tot), (float)MLP_S_MIN) : (float)MLP_S_MIN;
+            xr[3 * N2 + nd] = __float2bfloat16(0.25f * sf);
+            if (nd == 0) a.seta[e] = sf;
         }
-        __syncthreads();
-        if (live)
-            for (int f = 0; f < 3; ++f)
-                xr[f * N2 + nd] = __float2bfloat16((float)((v3[f] - st_mean[el][f]) * st_inv[el][f]));
-    }
-    if (live) {
         for (int c = 3 * N2 + 3 + nd; c < KP; c += N2) xr[c] = __float2bfloat16(0.0f);
-        if (nd == (GROUP ? 0 : 3)) {
+        if (nd == 0) {
             a.energy[e] = e2;
             a.ok[e] = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
         }
@@ -241,34 +222,42 @@ __global__ void __launch_bounds__(256) k_ind_features_warp(IndArgs a) {
         e2 += __shfl_xor_sync(0xffffffffu, e2, off);
     }
     fin = __all_sync(0xffffffffu, fin);
-    double d3[3] = {0.0, 0.0, 0.0};
+    // deviations from the (double) mean; their statistics in single
+    // precision, which is all the BF16 features need
+    float dv[3][R], d3[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
         m3[f] /= N2;
 #pragma unroll
-        for (int k = 0; k < R; ++k)
-            if (lane + 32 * k < N2) d3[f] += (v[f][k] - m3[f]) * (v[f][k] - m3[f]);
+        for (int k = 0; k < R; ++k) {
+            dv[f][k] = (lane + 32 * k < N2) ? (float)(v[f][k] - m3[f]) : 0.f;
+            d3[f] += dv[f][k] * dv[f][k];
+        }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
 #pragma unroll
         for (int f = 0; f < 3; ++f) d3[f] += __shfl_xor_sync(0xffffffffu, d3[f], off);
     __nv_bfloat16* xr = a.X + (long)e * KP;
+    float rmsf[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-        const double m = m3[f], rms = sqrt(d3[f] / N2);
-        const double inv = (rms > MLP_REL_FLAT * fabs(m) && rms > 0.0) ? 1.0 / rms : 0.0;
+        rmsf[f] = sqrtf(d3[f] * (1.0f / N2));
+        const float mf = fabsf((float)m3[f]);
+        const float inv = (rmsf[f] > (float)MLP_REL_FLAT * mf && rmsf[f] > 0.0f) ? 1.0f / rmsf[f] : 0.0f;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int p = lane + 32 * k;
-            if (p < N2) xr[f * N2 + p] = __float2bfloat16((float)((v[f][k] - m) * inv));
+            if (p < N2) xr[f * N2 + p] = __float2bfloat16(dv[f][k] * inv);
         }
-        if (lane == f) {
-            const double tot = m * m + rms * rms;
-            const double sf = (tot > 0.0 && rms > 0.0) ? fmax(log10(rms * rms / tot), MLP_S_MIN) : MLP_S_MIN;
-            xr[3 * N2 + f] = __float2bfloat16((float)(0.25 * sf));
-            if (f == 0) a.seta[e] = (float)sf;
-        }
+    }
+    if (lane < 3) {  // lanes 0, 1, 2: the scale feature of their field, one log10 pass
+        const float r = lane == 0 ? rmsf[0] : (lane == 1 ? rmsf[1] : rmsf[2]);
+        const float m = (float)(lane == 0 ? m3[0] : (lane == 1 ? m3[1] : m3[2]));
+        const float tot = m * m + r * r;
+        const float sf = (tot > 0.0f && r > 0.0f) ? fmaxf(log10f(r * r / tot), (float)MLP_S_MIN) : (float)MLP_S_MIN;
+        xr[3 * N2 + lane] = __float2bfloat16(0.25f * sf);
+        if (lane == 0) a.seta[e] = sf;
     }
     for (int c = 3 * N2 + 3 + lane; c < KP; c += 32) xr[c] = __float2bfloat16(0.0f);
     if (lane == 0) {

@@ -260,13 +260,34 @@ __device__ __forceinline__ void mlp_mma16816(float (&c)[4], unsigned a0, unsigne
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// The FP32 vectors a lane needs (biases and w3 at its fragment columns
+// 8 j + 2 t, 8 j + 2 t + 1), loaded once per warp.
+struct MlpLaneParams {
+    float b1[8], b2[8], w3[8], b3;
+};
+
+__device__ __forceinline__ MlpLaneParams mlp_lane_params(const float* __restrict__ P, const MlpLayout& L) {
+    MlpLaneParams r;
+    const int t = threadIdx.x & 3;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            r.b1[2 * j + k] = P[L.b1 + 8 * j + 2 * t + k];
+            r.b2[2 * j + k] = P[L.b2 + 8 * j + 2 * t + k];
+            r.w3[2 * j + k] = P[L.w3 + 8 * j + 2 * t + k];
+        }
+    r.b3 = P[L.b3];
+    return r;
+}
+
 // y for the 16 rows of X (bf16, shared, ld KP): lanes with t == 0 hold
 // y[g] in y_lo and y[g + 8] in y_hi (every lane of the quad has them).
-// W1 [32][KP], W2 [32][32] bf16 in shared memory; P the FP32 block.
+// W1 [32][KP], W2 [32][32] bf16 in shared memory.
 template <int KP>
 __device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, const __nv_bfloat16* W1,
-                                                      const __nv_bfloat16* W2, const float* __restrict__ P,
-                                                      const MlpLayout& L, float& y_lo, float& y_hi) {
+                                                      const __nv_bfloat16* W2, const MlpLaneParams& R,
+                                                      float& y_lo, float& y_hi) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const unsigned* Xu = reinterpret_cast<const unsigned*>(X);    // pairs of bf16
     const unsigned* W1u = reinterpret_cast<const unsigned*>(W1);
@@ -274,7 +295,7 @@ __device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, co
     float acc[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float b0 = P[L.b1 + 8 * j + 2 * t], b1v = P[L.b1 + 8 * j + 2 * t + 1];
+        const float b0 = R.b1[2 * j], b1v = R.b1[2 * j + 1];
         acc[j][0] = b0; acc[j][1] = b1v; acc[j][2] = b0; acc[j][3] = b1v;
     }
 #pragma unroll
@@ -291,7 +312,7 @@ __device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, co
     float acc2[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float b0 = P[L.b2 + 8 * j + 2 * t], b1v = P[L.b2 + 8 * j + 2 * t + 1];
+        const float b0 = R.b2[2 * j], b1v = R.b2[2 * j + 1];
         acc2[j][0] = b0; acc2[j][1] = b1v; acc2[j][2] = b0; acc2[j][3] = b1v;
     }
 #pragma unroll
@@ -312,7 +333,7 @@ __device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, co
     float lo = 0.f, hi = 0.f;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float w0 = P[L.w3 + 8 * j + 2 * t], w1 = P[L.w3 + 8 * j + 2 * t + 1];
+        const float w0 = R.w3[2 * j], w1 = R.w3[2 * j + 1];
         lo += fmaxf(acc2[j][0], 0.f) * w0 + fmaxf(acc2[j][1], 0.f) * w1;
         hi += fmaxf(acc2[j][2], 0.f) * w0 + fmaxf(acc2[j][3], 0.f) * w1;
     }
@@ -320,8 +341,8 @@ __device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, co
     lo += __shfl_xor_sync(0xffffffffu, lo, 2);
     hi += __shfl_xor_sync(0xffffffffu, hi, 1);
     hi += __shfl_xor_sync(0xffffffffu, hi, 2);
-    y_lo = lo + P[L.b3];
-    y_hi = hi + P[L.b3];
+    y_lo = lo + R.b3;
+    y_hi = hi + R.b3;
 }
 
 // Shared-memory carve-up of the MLP kernels (bytes): the BF16 weights once
@@ -334,6 +355,7 @@ struct MlpSmem {
     static constexpr int A1 = 16 * 32 * 2, Z = 16 * 32 * 4, G = 16 * 32 * 2, Y = 16 * 4;
     static constexpr int PER_WARP = XW + A1 + Z + 2 * G + Z + Y;
     static constexpr int bytes(int warps) { return W1 + W2 + warps * PER_WARP; }
+    static constexpr int fwd_bytes(int warps) { return W1 + W2 + warps * XW; }
 };
 
 __global__ void k_mlp_cast(int n, const float* __restrict__ P, __nv_bfloat16* __restrict__ Pb) {
@@ -362,7 +384,8 @@ __device__ __forceinline__ void mlp_load_rows(const __nv_bfloat16* __restrict__ 
 }
 
 // Network output y for M rows.  4 warps per block, grid-stride over 16-row
-// tiles; dynamic shared memory MlpSmem<KP>::bytes(4).
+// tiles; each warp holds its next tile in registers while it evaluates the
+// current one.  Dynamic shared memory MlpSmem<KP>::fwd_bytes(4).
 template <int KP>
 __global__ void __launch_bounds__(128) k_mlp_forward(int M, const __nv_bfloat16* __restrict__ X,
                                                      const float* __restrict__ P,
@@ -370,31 +393,44 @@ __global__ void __launch_bounds__(128) k_mlp_forward(int M, const __nv_bfloat16*
                                                      MlpLayout L, const int* __restrict__ Mlive = nullptr) {
     if (Mlive) M = min(M, *Mlive);  // rows past a live extent are skipped
     using S = MlpSmem<KP>;
+    constexpr int VPR = KP / 8;        // 16-byte vectors per row
+    constexpr int NV = 16 * VPR / 32;  // vectors per lane per tile
     extern __shared__ __align__(128) unsigned char mlp_smem[];
     __nv_bfloat16* sW1 = reinterpret_cast<__nv_bfloat16*>(mlp_smem);
     __nv_bfloat16* sW2 = reinterpret_cast<__nv_bfloat16*>(mlp_smem + S::W1);
     const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
-    unsigned char* mine = mlp_smem + S::W1 + S::W2 + w * S::PER_WARP;
-    __nv_bfloat16* sX = reinterpret_cast<__nv_bfloat16*>(mine);
-    __nv_bfloat16* a1b = reinterpret_cast<__nv_bfloat16*>(mine + S::XW);
-    float* z = reinterpret_cast<float*>(mine + S::XW + S::A1);
-    float* y16 = reinterpret_cast<float*>(mine + S::XW + S::A1 + S::Z + 2 * S::G + S::Z);
+    __nv_bfloat16* sX = reinterpret_cast<__nv_bfloat16*>(mlp_smem + S::W1 + S::W2 + w * S::XW);
     mlp_stage_weights(KP, Pb, L, sW1, sW2);
     __syncthreads();
+    if (M <= 0) return;
     const int tiles = (M + 15) / 16;
-    for (int t = blockIdx.x * 4 + w; t < tiles; t += gridDim.x * 4) {
-        const int r0 = t * 16;
-        mlp_load_rows<KP>(X, M, r0, sX);
+    const int stride = gridDim.x * 4;
+    auto fetch = [&](int t, uint4 (&buf)[NV]) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int i = lane + 32 * k;
+            const int r = min(t * 16 + i / VPR, M - 1);
+            buf[k] = reinterpret_cast<const uint4*>(X + (long)r * KP)[i % VPR];
+        }
+    };
+    const MlpLaneParams R = mlp_lane_params(P, L);
+    uint4 buf[NV];
+    int t = blockIdx.x * 4 + w;
+    if (t < tiles) fetch(t, buf);
+    for (; t < tiles; t += stride) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) reinterpret_cast<uint4*>(sX)[lane + 32 * k] = buf[k];
+        __syncwarp();
+        if (t + stride < tiles) fetch(t + stride, buf);  // in flight during this tile
         float ylo, yhi;
-        mlp_warp_forward_regs<KP>(sX, sW1, sW2, P, L, ylo, yhi);
-        const int g = lane >> 2;
+        mlp_warp_forward_regs<KP>(sX, sW1, sW2, R, ylo, yhi);
+        const int g = lane >> 2, r0 = t * 16;
         if ((lane & 3) == 0) {
             if (r0 + g < M) y[r0 + g] = ylo;
             if (r0 + g + 8 < M) y[r0 + g + 8] = yhi;
         }
-        __syncwarp();
+        __syncwarp();  // sX is rewritten next iteration
     }
-    (void)a1b; (void)z; (void)y16;
 }
 
 // Gradient of the loss (1/M) sum (y - t)^2 over M rows.  Each warp

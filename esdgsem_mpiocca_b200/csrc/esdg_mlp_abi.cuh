@@ -13,10 +13,11 @@ static bool mlp_ngl_ok(int ngl) { return ngl >= 3 && ngl <= 6; }
 template <int NGL>
 static cudaError_t mlp_set_smem() {
     constexpr int KP = mlp_kp(NGL);
-    const int bytes = MlpSmem<KP>::bytes(4);
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_forward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_forward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         MlpSmem<KP>::fwd_bytes(4));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mlp_backward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(k_mlp_backward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 MlpSmem<KP>::bytes(4));
     return e;
 }
 
@@ -85,7 +86,7 @@ int esdg_mlp_forward(int ngl, int M, const void* X, const float* P, const void* 
         constexpr int KP = mlp_kp(NG);                                                                      \
         e = mlp_set_smem<NG>();                                                                             \
         if (e == cudaSuccess)                                                                               \
-            k_mlp_forward<KP><<<blocks, 128, MlpSmem<KP>::bytes(4), s>>>(M, (const __nv_bfloat16*)X, P,     \
+            k_mlp_forward<KP><<<blocks, 128, MlpSmem<KP>::fwd_bytes(4), s>>>(M, (const __nv_bfloat16*)X, P, \
                                                                          (const __nv_bfloat16*)Pb, y, L); \
     }
     ESDG_MLP_DISPATCH(ngl, ESDG_F)
