@@ -355,6 +355,18 @@ class Engine {
             case 8: r = setup_tma<8>(); break;
         }
         if (r) return r;
+        if (AV) {  // grids of the sensor pass and the list kernels
+            switch (ngl) {
+                case 2: r = setup_indicator<2>(); break;
+                case 3: r = setup_indicator<3>(); break;
+                case 4: r = setup_indicator<4>(); break;
+                case 5: r = setup_indicator<5>(); break;
+                case 6: r = setup_indicator<6>(); break;
+                case 7: r = setup_indicator<7>(); break;
+                case 8: r = setup_indicator<8>(); break;
+            }
+            if (r) return r;
+        }
         built = true;
         return 0;
     }
@@ -386,7 +398,8 @@ class Engine {
         a.B = B; a.D = D; a.Dhat = Dhat; a.Dstrong = Dstrong; a.Vinv = Vinv; a.SP = SP; a.SGX = SGX; a.SGY = SGY;
         a.SPV = SPV; a.side = side; a.q = q; a.gRK = gRK; a.Qt = Qt; a.Qtmp = Qtmp; a.GX = GX; a.GY = GY; a.VP = VP;
         a.elem_inst = elem_inst; a.st = st; a.rkA = A; a.rkB = Bc; a.rkC = C; a.mode = mode; a.lam = lam;
-        a.shock = shock; a.c = phys(); a.extent = extent;
+        (void)shock;
+        a.c = phys(); a.extent = extent;
         return a;
     }
 
@@ -532,8 +545,12 @@ class Engine {
             launch_face<NGL>(false);
             launch_elem_plain<NGL>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
         } else {
+            // the reference path: the sensor (same arithmetic as okl/ShockCapturing,
+            // one entry of the modal transform per thread) then the viscous
+            // terms on every element
+            if (shock_stage) launch_indicator<NGL>(0);
             launch_face<NGL>(true);
-            k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0, shock_stage ? 1 : 0));
+            k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0, 0));
             const long n = (long)F * NGL;
             k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
                                                                          elem_inst, st, geomFace);
@@ -554,17 +571,12 @@ class Engine {
         ++launches;
     }
 
-    template <int NGL>
-    void launch_shock() {
-        k_shock<NGL><<<(K + 7) / 8, 256, 0, stream>>>(K, q, B, Vinv, VP, elem_inst, st, phys());
-        ++launches;
-    }
 
     template <int NGL>
     void launch_indicator(int stage0) {
-        cudaMemsetAsync(act, 0, (size_t)(K + 1) * sizeof(int), stream);
+        if (indicator) cudaMemsetAsync(act, 0, (size_t)(K + 1) * sizeof(int), stream);
         IndArgs ia;
-        ia.K = K; ia.q = q; ia.B = B; ia.Vinv = Vinv; ia.VP = VP; ia.act = act; ia.nbr = nbr;
+        ia.K = K; ia.q = q; ia.B = B; ia.Vinv = Vinv; ia.VP = VP; ia.act = indicator ? act : nullptr; ia.nbr = nbr;
         ia.elem_inst = elem_inst; ia.st = st; ia.c = phys(); ia.stage0 = stage0;
         ia.P = mlpP; ia.Pb = mlpPb; ia.L = mlp_layout(NGL); ia.margin = ind_margin;
         ia.emin = ind_emin; ia.emax = ind_emax; ia.stats = ind_stats; ia.extent = extent;
@@ -643,16 +655,6 @@ class Engine {
             cudaError_t e = cudaDeviceSynchronize();
             if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
             k_build_nbr<<<(K + 255) / 256, 256, 0, stream>>>(0, K, side, ftab, nbr);
-            switch (ngl) {
-                case 2: r = setup_indicator<2>(); break;
-                case 3: r = setup_indicator<3>(); break;
-                case 4: r = setup_indicator<4>(); break;
-                case 5: r = setup_indicator<5>(); break;
-                case 6: r = setup_indicator<6>(); break;
-                case 7: r = setup_indicator<7>(); break;
-                case 8: r = setup_indicator<8>(); break;
-            }
-            if (r) return r;
         }
         if (mode == 2) {
             const int n = mlp_layout(ngl).total;
@@ -697,10 +699,7 @@ class Engine {
 
     template <int NGL>
     void launch_step() {
-        if (AV) {
-            if (indicator) launch_indicator<NGL>(1);
-            else launch_shock<NGL>();
-        }
+        if (AV) launch_indicator<NGL>(1);
         k_step_begin<<<(I + 127) / 128, 128, 0, stream>>>(I, st, ngl, AV);
         ++launches;
         if (rkSSP) {
@@ -861,7 +860,7 @@ class Engine {
 
     template <int NGL>
     void launch_step_profiled(double* face_ms, double* elem_ms) {
-        if (AV) launch_shock<NGL>();
+        if (AV) launch_indicator<NGL>(1);
         k_step_begin<<<(I + 127) / 128, 128, 0, stream>>>(I, st, ngl, AV);
         ++launches;
         if (rkSSP)
@@ -878,7 +877,8 @@ class Engine {
             if (!AV) {
                 launch_elem_plain<NGL>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
             } else {
-                k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0, s > 0));
+                if (s > 0) launch_indicator<NGL>(0);
+                k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0, 0));
                 const long n = (long)F * NGL;
                 k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
                                                                              elem_inst, st, geomFace);

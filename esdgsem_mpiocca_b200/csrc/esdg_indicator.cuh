@@ -3,8 +3,9 @@
 // on every element).
 //
 // Per element e it writes the artificial viscosity VP[e] and, where
-// VP[e] > 0, flags e and its face neighbours in act[] (zeroed before the
-// launch).  The viscous terms of an element vanish exactly unless it or a
+// VP[e] > 0 and an active set is kept (act non-null), flags e and its face
+// neighbours in act[] (zeroed before the launch).  Without act it is the
+// reference path's sensor pass.  The viscous terms of an element vanish exactly unless it or a
 // neighbour has VP > 0 (the face viscosity is max(VP_L, VP_R), the volume
 // term is VP_e times the gradient), so the stage's viscous kernels run on
 // the flagged elements only and give the same numbers as on all of them.
@@ -294,7 +295,7 @@ __device__ __forceinline__ IndLoad ind_load(const IndArgs& a, int t) {
         L.h = a.q[(long)e * 3 * N2 + nd];
         L.b = a.B[(long)e * N2 + nd];
         L.ins = inst_of(a.elem_inst, e);
-        if (nd == 0) L.nb = a.nbr[e];
+        if (nd == 0 && a.act) L.nb = a.nbr[e];
     }
     return L;
 }
@@ -394,7 +395,8 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
             }
             a.VP[e] = v;
             if (a.stage0 && v > 0.0) atomicMax(&a.st[cur.ins].visc_key, dbl_key(v));
-            if (!(v <= 0.0)) mark_active(a.act, e, cur.nb);  // NaN flags too: its viscous path runs as on the full path
+            // NaN flags too: its viscous path runs as on the full path
+            if (a.act && !(v <= 0.0)) mark_active(a.act, e, cur.nb);
             cnt[kind] += 1;
             if (!(v <= 0.0)) cnt[3] += 1;
         }

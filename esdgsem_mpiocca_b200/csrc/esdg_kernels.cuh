@@ -8,9 +8,10 @@
 //                differencing volume integral, lifting of the four face
 //                fluxes, low-storage (or SSP) RK update and, on the last
 //                stage, the element wave-speed maximum for the next dt.
-// With artificial viscosity (BR1 gradient + viscous terms) a stage is four
-// launches: face_flux (+ gradient face flux), element_av1 (inviscid Qt,
-// shock sensor, lifted gradient), face_visc, element_av2 (viscous volume and
+// With artificial viscosity (BR1 gradient + viscous terms) a stage is the
+// sensor pass (esdg_indicator.cuh; at the step start and before stages > 0)
+// and four launches: face_flux (+ gradient face flux), element_av1 (inviscid
+// Qt and the lifted gradient), face_visc, element_av2 (viscous volume and
 // lift + RK update).
 #pragma once
 
@@ -85,7 +86,6 @@ struct ElemArgs {
     double rkA, rkB, rkC;
     int mode;        // 0: LS-RK update, 1: SSP update, 2: write Qt only
     int lam;         // 1: element wave speed max into st[inst].lam_key after the update
-    int shock;       // AV: recompute the shock sensor into VP
     PhysConst c;
     // Active set (null: none).  Plain element kernels write Qt instead of
     // updating flagged elements and append them to alist (count in
@@ -420,44 +420,7 @@ __device__ __forceinline__ double sensor_w(const double* V, const double* M1, in
     return acc;
 }
 
-// Modal energy sensor of one element (okl/ShockCapturing/ShockCapturing.okl:17-234),
-// evaluated by one thread; m = (h+b) nodal values [eta][xi], V = VdmInv
-// row-major [mode][node]; w receives the modal coefficients [mode_xi][mode_eta].
-template <int NGL>
-__device__ double shock_sensor(const PhysConst& c, const double* m, const double* V, double* w) {
-    double M1[NGL * NGL];
-    for (int i = 0; i < NGL; ++i)
-        for (int j = 0; j < NGL; ++j) M1[i * NGL + j] = sensor_m1<NGL>(V, m, i, j);
-    for (int i = 0; i < NGL; ++i)
-        for (int j = 0; j < NGL; ++j) w[i * NGL + j] = sensor_w<NGL>(V, M1, i, j);
-    return sensor_tail<NGL>(c, w);
-}
-
-// Shock sensor for every element and the per-instance maximum viscosity
-// (src/deviceclass.cpp:914-924).  One element per warp.
-template <int NGL>
-__global__ void __launch_bounds__(256) k_shock(int K, const double* __restrict__ q, const double* __restrict__ B,
-                                               const double* __restrict__ Vinv, double* __restrict__ VP,
-                                               const int* __restrict__ elem_inst, DevState* st, PhysConst c) {
-    constexpr int N2 = NGL * NGL;
-    __shared__ double sm[8][N2], sw[8][N2], sV[N2];
-    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
-    if (threadIdx.x < N2) sV[threadIdx.x] = Vinv[threadIdx.x];
-    __syncthreads();
-    const int e = blockIdx.x * 8 + w;
-    if (e >= K) return;
-    const int ins = inst_of(elem_inst, e);
-    if (st[ins].done) return;
-    for (int p = lane; p < N2; p += 32) sm[w][p] = B[(long)e * N2 + p] + q[(long)e * 3 * N2 + p];
-    __syncwarp();
-    if (lane == 0) {
-        const double v = shock_sensor<NGL>(c, sm[w], sV, sw[w]);
-        VP[e] = v;
-        atomicMax(&st[ins].visc_key, dbl_key(v));
-    }
-}
-
-// Inviscid volume + lift written to Qt, shock sensor (stages > 0) and the
+// Inviscid volume + lift written to Qt and the
 // lifted, h-scaled BR1 gradient of the velocities.
 // okl/BR1_Gradient/calcGradient.okl:18-156, SurfaceKernelGradient.okl:16-150,
 // scaleGradient.okl:17-60.
@@ -566,13 +529,6 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av1(ElemArg
         const long gid = (long)e * 2 * N2 + nd;
         a.GX[gid] = h * gx0; a.GX[gid + N2] = h * gx1;
         a.GY[gid] = h * gy0; a.GY[gid + N2] = h * gy1;
-    }
-    if (a.shock && nd == 0) {
-        // (h + b) of this element; sh is not written after the staging sync.
-        double m[N2], w[N2];
-        for (int p = 0; p < N2; ++p) m[p] = a.B[(long)e * N2 + p] + sh[el * N2 + p];
-        const double v = shock_sensor<NGL>(a.c, m, sV, w);
-        a.VP[e] = v;
     }
 }
 
