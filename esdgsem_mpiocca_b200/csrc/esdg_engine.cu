@@ -392,13 +392,12 @@ class Engine {
         return 0;
     }
 
-    ElemArgs elem_args(int mode, double A, double Bc, double C, int lam, int shock) {
+    ElemArgs elem_args(int mode, double A, double Bc, double C, int lam) {
         ElemArgs a;
         a.K = K; a.Jinv = Jinv; a.Yxi = Yxi; a.Yeta = Yeta; a.Xxi = Xxi; a.Xeta = Xeta; a.Bx = Bx; a.By = By;
         a.B = B; a.D = D; a.Dhat = Dhat; a.Dstrong = Dstrong; a.Vinv = Vinv; a.SP = SP; a.SGX = SGX; a.SGY = SGY;
         a.SPV = SPV; a.side = side; a.q = q; a.gRK = gRK; a.Qt = Qt; a.Qtmp = Qtmp; a.GX = GX; a.GY = GY; a.VP = VP;
         a.elem_inst = elem_inst; a.st = st; a.rkA = A; a.rkB = Bc; a.rkC = C; a.mode = mode; a.lam = lam;
-        (void)shock;
         a.c = phys(); a.extent = extent;
         return a;
     }
@@ -501,7 +500,7 @@ class Engine {
             for (auto& b2 : a2)
                 for (auto& c2 : b2) cudaEventCreate(&c2);
         const bool have = gStages > 0;
-        ElemArgs ea = elem_args(rkSSP ? 1 : 0, have ? gA[0] : 0.0, have ? gB[0] : 1.0, have ? gC[0] : 0.0, 0, 0);
+        ElemArgs ea = elem_args(rkSSP ? 1 : 0, have ? gA[0] : 0.0, have ? gB[0] : 1.0, have ? gC[0] : 0.0, 0);
         ea.q = tq;
         ea.gRK = tg;
         for (int v = 0; v < TMA_VARIANTS; ++v)
@@ -552,7 +551,7 @@ class Engine {
             // viscous update over the list
             if (shock_stage) launch_indicator<NGL>(0);
             launch_face<NGL>(true);
-            ElemArgs ea = elem_args(mode, A, Bc, C, lam_in_elem, 0);
+            ElemArgs ea = elem_args(mode, A, Bc, C, lam_in_elem);
             ea.act = act; ea.alist = alist; ea.acount = act + K;
             launch_elem_plain<NGL>(ea);
             k_grad_list<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
@@ -563,18 +562,18 @@ class Engine {
             launches += 3;
         } else if (!AV) {
             launch_face<NGL>(false);
-            launch_elem_plain<NGL>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
+            launch_elem_plain<NGL>(elem_args(mode, A, Bc, C, lam_in_elem));
         } else {
             // the reference path: the sensor (same arithmetic as okl/ShockCapturing,
             // one entry of the modal transform per thread) then the viscous
             // terms on every element
             if (shock_stage) launch_indicator<NGL>(0);
             launch_face<NGL>(true);
-            k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0, 0));
+            k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0));
             const long n = (long)F * NGL;
             k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
                                                                          elem_inst, st, geomFace);
-            k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, A, Bc, C, lam_in_elem, 0));
+            k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, A, Bc, C, lam_in_elem));
             launches += 3;
         }
         if (PP && mode != 2) {
@@ -895,14 +894,14 @@ class Engine {
             launch_face<NGL>(AV != 0);
             cudaEventRecord(pev[1], stream);
             if (!AV) {
-                launch_elem_plain<NGL>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
+                launch_elem_plain<NGL>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem));
             } else {
                 if (s > 0) launch_indicator<NGL>(0);
-                k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0, 0));
+                k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0));
                 const long n = (long)F * NGL;
                 k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
                                                                              elem_inst, st, geomFace);
-                k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem, 0));
+                k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem));
                 launches += 3;
             }
             cudaEventRecord(pev[2], stream);

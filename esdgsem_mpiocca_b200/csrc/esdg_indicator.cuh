@@ -91,8 +91,6 @@ __device__ __forceinline__ void mark_active(int* act, int e, int4 nb) {
 template <int NGL>
 struct IndShape {
     static constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE, THREADS = NE * N2;
-    static constexpr int KP = mlp_kp(NGL);
-    static constexpr int ROWS = 16;  // feature rows per block (NE <= 16 for NGL >= 4)
 };
 
 
@@ -136,7 +134,7 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs
         const double v3[3] = {cur.b + cur.h, cur.hu, cur.hv};
         double mh = cur.h, e2 = v3[0] * v3[0];
         bool fin = isfinite(cur.h) && isfinite(cur.hu) && isfinite(cur.hv);
-        double m3[3] = {v3[0], v3[1], v3[2]}, d3[3];
+        double m3[3] = {v3[0], v3[1], v3[2]};
 #pragma unroll
         for (int off = N2 / 2; off > 0; off >>= 1) {
 #pragma unroll
@@ -158,7 +156,6 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs
         for (int off = N2 / 2; off > 0; off >>= 1)
 #pragma unroll
             for (int f = 0; f < 3; ++f) d3f[f] += __shfl_xor_sync(0xffffffffu, d3f[f], off);
-        (void)d3;
         if (!live) continue;  // after the shuffles: the whole group skips together
         __nv_bfloat16* xr = a.X + (long)e * KP;
         float rmsf[3];
