@@ -138,6 +138,46 @@ def test_lake_at_rest_curved():
         assert np.abs(q[:, v]).max() <= 10 * drift + 1e-15, (v, np.abs(q[:, v]).max(), drift)
 
 
+def _lake(nel, steps, oracle=False):
+    pr = problems.curved_lake(N=4, nel=nel, seed=0, ripple=0.0, steps=steps)
+    s = Solver(pr)
+    try:
+        s.run()
+        q = s.q().reshape(pr.K, 3, -1)
+    finally:
+        s.close()
+    ref = OracleProblem(pr).run()["q"].reshape(pr.K, 3, -1) if oracle else None
+    return q, pr.b.reshape(pr.K, -1), ref
+
+
+def test_lake_at_rest_128_matches_oracle_bitwise():
+    """The benchmark's bumps and mapping at 128x128 elements, 100 steps: the
+    engine's state equals the oracle's bit for bit, so its departure from
+    rest is the scheme's own round-off and not the engine's."""
+    q, b, ref = _lake(128, 100, oracle=True)
+    assert np.array_equal(q, ref)
+    assert np.abs(q[:, 0] + b - 1.0).max() <= 5e-13
+
+
+def test_lake_at_rest_full_size():
+    """The benchmark mesh at rest (512x512 curved, N=4, 8 bumps).  The
+    scheme's round-off in the balance of flux and bathymetry terms scales
+    with the terms, ~1/dx: max|h+b-1| is 1.3e-13 at 64x64 elements and
+    1.26e-12 at 512x512 in the oracle's arithmetic (equal to the engine's,
+    see the 128x128 test).  Checked here: the surface error stays at that
+    level and does not grow from step 20 to step 100, and the momentum grows
+    at most linearly at the round-off rate (about 2.5e-12 per step)."""
+    q20, b, _ = _lake(512, 20)
+    q100, _, _ = _lake(512, 100)
+    e20 = np.abs(q20[:, 0] + b - 1.0).max()
+    e100 = np.abs(q100[:, 0] + b - 1.0).max()
+    assert e100 <= 2e-12, e100
+    assert e100 <= 1.1 * e20, (e20, e100)
+    m20, m100 = np.abs(q20[:, 1:]).max(), np.abs(q100[:, 1:]).max()
+    assert m100 <= 5e-12 * 100, m100
+    assert m100 <= 1.2 * 5 * m20, (m20, m100)
+
+
 def test_ssp_rk3_matches_oracle():
     pr = problems.periodic_bump(NumFlux=0, steps=40)
     pr.params.rkOrder, pr.params.rkSSP = 3, 1
