@@ -44,6 +44,18 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+# element-kernel variants of the engine at N = 4 (index = variant number)
+ELEMENT_KERNELS_N4 = ("k_element_tma<5,2,2>", "k_element_tma<5,3,2>", "k_element_tma<5,2,3>",
+                      "k_element_rows<5,32,2,1>", "k_element_rows<5,16,2,2>")
+
+
+def element_kernel_name(dc):
+    ev = dc.element_variants()
+    if not ev or ev["chosen"] < 0:
+        return "k_element<5>"
+    return ELEMENT_KERNELS_N4[ev["chosen"]]
+
+
 def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
     """The maximum of x over all ranks (x itself without a process group)."""
     if dist is None:
@@ -268,7 +280,7 @@ def main():
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded curved_lake generator; no dataset exists)",
         "config": workload_config(prob, {"sim_time_reached": t_sim}),
-        "roofline": {"bound": "hbm", "kernel": "k_element_tma<5>", "achieved": ach, "peak": hbm, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": element_kernel_name(s.dc), "achieved": ach, "peak": hbm, "unit": "GB/s",
                      "frac": ach / hbm, "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                      "traffic": traffic,
                      "bytes_per_node": ELEM_BYTES_PER_NODE, "launch_ms": kern["ms"],
@@ -277,7 +289,7 @@ def main():
                                "achieved": STAGE_BYTES_PER_NODE * prob.dofs() * STAGES * args.steps /
                                (ms_max / 1e3) / 1e9}},
         "e2e": e2e,
-        "autotuned": s.dc.tuned_config(),
+        "autotuned": s.dc.element_variants(),
         "gpu_launches": int(launches),
         "clocks": ck.result,
     }

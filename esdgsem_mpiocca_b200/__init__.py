@@ -74,6 +74,10 @@ def _declare(lib):
         "esdg_ensemble_destroy": (_I, [_VP]),
         "esdg_state_pointers": (_I, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
         "esdg_tuned_config": (_I, [_VP, _PI, _PI, ctypes.POINTER(ctypes.c_float)]),
+        "esdg_element_variants": (_I, [_VP, _PI, _PI, ctypes.POINTER(ctypes.c_float), _PI, _I]),
+        "esdg_set_element_variant": (_I, [_VP, _I]),
+        "esdg_ensemble_element_variants": (_I, [_VP, _PI, _PI, ctypes.POINTER(ctypes.c_float), _PI, _I]),
+        "esdg_ensemble_set_element_variant": (_I, [_VP, _I]),
         "esdg_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),
         "esdg_indicator_stats": (_I, [_VP, ctypes.POINTER(ctypes.c_ulonglong), _I]),
         "esdg_ensemble_set_indicator": (_I, [_VP, _I, ctypes.POINTER(ctypes.c_float), _I, ctypes.c_float]),

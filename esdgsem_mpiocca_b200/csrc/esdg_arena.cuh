@@ -100,6 +100,7 @@ class Arena : public Engine {
             (r = h2d(GLw, B.wGL.data(), B.wGL.size(), "GLw")))
             return r;
         Vinv_h = B.VdmInv;
+        Dfd_h = B.D;
         copied = true;
         if ((r = build(1, NumFlux_, rkSSP_, AV_, PP_, 0, 0))) return r;
         double A[8], Bc[8], C[8];
@@ -403,6 +404,18 @@ int esdg_ensemble_set_stream(esdg_ensemble* en, void* cuda_stream) {
     cudaSetDevice(en->a.device);
     en->a.stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : en->a.own_stream;
     return en->a.capture_step_graph();
+}
+
+int esdg_ensemble_set_element_variant(esdg_ensemble* en, int variant) {
+    if (!en) return ESDG_E_ARG;
+    cudaSetDevice(en->a.device);
+    return en->a.set_element_variant(variant);
+}
+
+int esdg_ensemble_element_variants(const esdg_ensemble* en, int* chosen, int* count, float* ms, int* ctas_per_sm,
+                                   int cap) {
+    if (!en) return ESDG_E_ARG;
+    return element_variants(en->a, chosen, count, ms, ctas_per_sm, cap);
 }
 
 int esdg_ensemble_set_indicator(esdg_ensemble* en, int mode, const float* params, int nparams, float margin) {

@@ -28,6 +28,7 @@
 #include "../../include/esdg_b200.h"
 #include "esdg_kernels.cuh"
 #include "esdg_tma.cuh"
+#include "esdg_rows.cuh"
 #include "esdg_indicator.cuh"
 #include "esdg_setup.hpp"
 
@@ -150,6 +151,7 @@ class Engine {
     int* extent = nullptr;                    // arena: live extent {elements, faces} (null: all)
     unsigned long long* ind_stats = nullptr;  // [4] decision counts
     std::vector<double> Vinv_h;
+    std::vector<double> Dfd_h;  // flux-differencing matrix (host copy, row kernel parameter)
     int list_grid = 0;                        // persistent grid of the list kernels
     int ind_grid[2] = {1, 1};                 // persistent grids of the indicator (modal, learned)
 
@@ -325,6 +327,7 @@ class Engine {
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "copyDeviceVariables");
         Vinv_h.assign(Vinv_h_, Vinv_h_ + n2);
+        Dfd_h.assign(D_h, D_h + n2);
         copied = true;
         return 0;
     }
@@ -402,13 +405,19 @@ class Engine {
         return a;
     }
 
-    // Plain-path element kernel: the TMA-pipelined persistent kernel when the
-    // element count allows 16-byte bulk granularity, else the one-shot one.
-    // Its occupancy variant (tma_min_blocks) is picked by timing on the mesh.
-    int tma_grid[TMA_VARIANTS] = {0, 0, 0};  // persistent grid sizes (0: not usable)
+    // Plain-path element kernel: a persistent bulk-copy-pipelined kernel when
+    // the element count allows 16-byte bulk granularity, else the one-shot
+    // one.  Variants 0..TMA_VARIANTS-1: node-per-thread k_element_tma (CTAs
+    // per SM, pipeline depth); then ROW_VARIANTS line-per-thread
+    // k_element_rows (elements per tile).  The autotuner times them on the
+    // mesh; esdg_set_element_variant can fix one.
+    static constexpr int ELEM_VARIANTS = TMA_VARIANTS + ROW_VARIANTS;
+    int tma_grid[ELEM_VARIANTS] = {};  // persistent grid sizes (0: not usable)
+    int tma_ctas[ELEM_VARIANTS] = {};  // resident CTAs per SM
     int tma_variant = 0;
+    int forced_variant = -1;
     bool tma_tuned = false;
-    float tma_tune_ms[TMA_VARIANTS] = {0.0f, 0.0f, 0.0f};
+    float tma_tune_ms[ELEM_VARIANTS] = {};
 
     template <int NGL, int V>
     int setup_tma_variant() {
@@ -423,6 +432,25 @@ class Engine {
         if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
         const int ntiles = (K + T::NE - 1) / T::NE;
         tma_grid[V] = std::max(1, std::min(ntiles, std::max(per_sm, 1) * sms));
+        tma_ctas[V] = per_sm;
+        return 0;
+    }
+
+    template <int NGL, int R>
+    int setup_row_variant() {
+        constexpr int NE = row_ne(NGL, R);
+        using T = RowShape<NGL, NE, 2>;
+        auto kern = k_element_rows<NGL, NE, 2, row_min_blocks(R)>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T::THREADS, T::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+        const int ntiles = (K + NE - 1) / NE;
+        tma_grid[TMA_VARIANTS + R] = per_sm > 0 ? std::max(1, std::min(ntiles, per_sm * sms)) : 0;
+        tma_ctas[TMA_VARIANTS + R] = per_sm;
         return 0;
     }
 
@@ -430,12 +458,17 @@ class Engine {
     int setup_tma() {
         using T = TmaShape<NGL>;
         for (auto& g : tma_grid) g = 0;
+        for (auto& c : tma_ctas) c = 0;
         tma_tuned = false;
         tma_variant = 0;
         if (((long long)K * T::N2) % 2 != 0) return 0;
         int r = setup_tma_variant<NGL, 0>();
         if (!r) r = setup_tma_variant<NGL, 1>();
         if (!r) r = setup_tma_variant<NGL, 2>();
+        if constexpr (row_ngl_ok(NGL)) {
+            if (!r) r = setup_row_variant<NGL, 0>();
+            if (!r) r = setup_row_variant<NGL, 1>();
+        }
         return r;
     }
 
@@ -446,11 +479,26 @@ class Engine {
         k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
     }
 
+    template <int NGL, int R>
+    void launch_rows_v(const ElemArgs& ea) {
+        if constexpr (row_ngl_ok(NGL)) {
+            constexpr int NE = row_ne(NGL, R);
+            using T = RowShape<NGL, NE, 2>;
+            DLine<NGL> dm;
+            for (int i = 0; i < NGL * NGL; ++i) dm.v[i] = Dfd_h[i];
+            const int ntiles = (K + NE - 1) / NE;
+            k_element_rows<NGL, NE, 2, row_min_blocks(R)>
+                <<<tma_grid[TMA_VARIANTS + R], T::THREADS, T::SMEM, stream>>>(ea, dm, ntiles);
+        }
+    }
+
     template <int NGL>
     void launch_tma(const ElemArgs& ea, int v) {
         if (v == 0) launch_tma_v<NGL, 0>(ea);
         else if (v == 1) launch_tma_v<NGL, 1>(ea);
-        else launch_tma_v<NGL, 2>(ea);
+        else if (v == 2) launch_tma_v<NGL, 2>(ea);
+        else if (v == TMA_VARIANTS) launch_rows_v<NGL, 0>(ea);
+        else launch_rows_v<NGL, 1>(ea);
     }
 
     template <int NGL>
@@ -475,6 +523,10 @@ class Engine {
         if (tma_tuned) return 0;
         tma_tuned = true;
         if (tma_grid[0] <= 0) return 0;
+        if (forced_variant >= 0) {
+            tma_variant = forced_variant;
+            return 0;
+        }
         const int Kt = tune_K >= 0 ? tune_K : K;
         if (Kt <= 0) return 0;
         const size_t nd = (size_t)Kt * NGL * NGL * 3;
@@ -495,7 +547,7 @@ class Engine {
         cudaMemcpyAsync(tq, q, nd * sizeof(double), cudaMemcpyDeviceToDevice, stream);
         cudaMemcpyAsync(tg, gRK, nd * sizeof(double), cudaMemcpyDeviceToDevice, stream);
         constexpr int REPS = 5;
-        cudaEvent_t ev[TMA_VARIANTS][REPS][2];
+        cudaEvent_t ev[ELEM_VARIANTS][REPS][2];
         for (auto& a2 : ev)
             for (auto& b2 : a2)
                 for (auto& c2 : b2) cudaEventCreate(&c2);
@@ -503,10 +555,10 @@ class Engine {
         ElemArgs ea = elem_args(rkSSP ? 1 : 0, have ? gA[0] : 0.0, have ? gB[0] : 1.0, have ? gC[0] : 0.0, 0);
         ea.q = tq;
         ea.gRK = tg;
-        for (int v = 0; v < TMA_VARIANTS; ++v)
+        for (int v = 0; v < ELEM_VARIANTS; ++v)
             if (tma_grid[v] > 0) launch_tma<NGL>(ea, v);  // first-launch costs
         for (int r = 0; r < REPS; ++r)
-            for (int v = 0; v < TMA_VARIANTS; ++v) {
+            for (int v = 0; v < ELEM_VARIANTS; ++v) {
                 if (tma_grid[v] <= 0) continue;
                 cudaMemsetAsync(flush, r + v, flush_bytes, stream);
                 cudaEventRecord(ev[v][r][0], stream);
@@ -515,7 +567,7 @@ class Engine {
             }
         cudaError_t e = cudaStreamSynchronize(stream);
         float best = 1e30f;
-        for (int v = 0; v < TMA_VARIANTS && e == cudaSuccess; ++v) {
+        for (int v = 0; v < ELEM_VARIANTS && e == cudaSuccess; ++v) {
             if (tma_grid[v] <= 0) continue;
             float sum = 0.0f;
             for (int r = 0; r < REPS && e == cudaSuccess; ++r) {
@@ -751,6 +803,19 @@ class Engine {
 
     int check_ready() {
         if (!inited || !copied || !built) return fail(ESDG_E_ARG, "call initDeviceVariables, copyDeviceVariables and buildDeviceKernels first");
+        return 0;
+    }
+
+    // Fixes the element-kernel variant (-1: let the autotuner pick).
+    int set_element_variant(int v) {
+        if (!built) return fail(ESDG_E_ARG, "set_element_variant before buildDeviceKernels");
+        if (v < -1 || v >= ELEM_VARIANTS) return fail(ESDG_E_ARG, "element variant out of range");
+        if (v >= 0 && tma_grid[v] <= 0)
+            return fail(ESDG_E_UNSUPPORTED, "element variant not available for this degree and element count");
+        forced_variant = v;
+        tma_tuned = v >= 0;
+        if (v >= 0) tma_variant = v;
+        if (graph) return capture_step_graph();
         return 0;
     }
 
@@ -1163,14 +1228,38 @@ int esdg_indicator_stats(esdg_deviceclass* d, unsigned long long* counts4, int r
     return d->eng.indicator_stats(counts4, reset);
 }
 
-int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, int* stages, float* ms_variants2) {
+int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, int* stages, float* ms_variants3) {
     if (!d) return ESDG_E_ARG;
     const esdg::Engine& E = d->eng;
-    if (ctas_per_sm) *ctas_per_sm = E.tma_grid[E.tma_variant] > 0 ? esdg::tma_min_blocks(E.tma_variant) : 0;
-    if (ms_variants2)
-        for (int v = 0; v < esdg::TMA_VARIANTS; ++v) ms_variants2[v] = E.tma_tune_ms[v];
-    if (stages) *stages = E.tma_grid[E.tma_variant] > 0 ? esdg::tma_stages(E.tma_variant) : 0;
+    const int v = E.tma_variant;
+    const bool node_kernel = v < esdg::TMA_VARIANTS;
+    if (ctas_per_sm) *ctas_per_sm = E.tma_grid[v] > 0 ? (node_kernel ? esdg::tma_min_blocks(v) : E.tma_ctas[v]) : 0;
+    if (ms_variants3)
+        for (int k = 0; k < esdg::TMA_VARIANTS; ++k) ms_variants3[k] = E.tma_tune_ms[k];
+    if (stages) *stages = E.tma_grid[v] > 0 ? (node_kernel ? esdg::tma_stages(v) : 2) : 0;
     return E.tma_tuned ? ESDG_OK : ESDG_E_ARG;
+}
+
+static int element_variants(const esdg::Engine& E, int* chosen, int* count, float* ms, int* ctas, int cap) {
+    constexpr int NV = esdg::Engine::ELEM_VARIANTS;
+    if (count) *count = NV;
+    if (chosen) *chosen = E.tma_grid[E.tma_variant] > 0 ? E.tma_variant : -1;
+    for (int k = 0; k < NV && k < cap; ++k) {
+        if (ms) ms[k] = E.tma_tune_ms[k];
+        if (ctas) ctas[k] = E.tma_grid[k] > 0 ? E.tma_ctas[k] : 0;
+    }
+    return E.tma_tuned ? ESDG_OK : ESDG_E_ARG;
+}
+
+int esdg_element_variants(const esdg_deviceclass* d, int* chosen, int* count, float* ms, int* ctas_per_sm,
+                          int cap) {
+    if (!d) return ESDG_E_ARG;
+    return element_variants(d->eng, chosen, count, ms, ctas_per_sm, cap);
+}
+
+int esdg_set_element_variant(esdg_deviceclass* d, int variant) {
+    ESDG_GUARD(d);
+    return d->eng.set_element_variant(variant);
 }
 
 int esdg_state_pointers(esdg_deviceclass* d, const double** q, const double** b, const double** VdmInv) {

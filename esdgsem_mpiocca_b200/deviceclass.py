@@ -29,6 +29,18 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+def _element_variants(L, fn, h, cap=8):
+    chosen, count = ctypes.c_int(), ctypes.c_int()
+    ms = (ctypes.c_float * cap)()
+    ctas = (ctypes.c_int * cap)()
+    rc = fn(h, ctypes.byref(chosen), ctypes.byref(count), ms, ctas, cap)
+    if rc != 0:
+        return None
+    n = min(count.value, cap)
+    return {"chosen": chosen.value, "count": count.value, "ms": [float(v) for v in ms[:n]],
+            "ctas_per_sm": [int(v) for v in ctas[:n]]}
+
+
 def _indicator_params(net):
     if net is None:
         raise ValueError("the learned indicator needs a network")
@@ -158,6 +170,16 @@ class DeviceClass:
         rc = self._L.esdg_tuned_config(self.h, ctypes.byref(c), ctypes.byref(st), ms)
         return None if rc != 0 else {"ctas_per_sm": c.value, "stages": st.value,
                                      "variant_ms": [float(v) for v in ms]}
+
+    def element_variants(self):
+        """All element-kernel variants: the one in use, the autotuner's
+        launch times (ms, 0 if not timed) and resident CTAs per SM (0: not
+        available here); None before the tuning ran."""
+        return _element_variants(self._L, self._L.esdg_element_variants, self.h)
+
+    def set_element_variant(self, variant: int):
+        """Fixes the element-kernel variant (-1: the autotuner's choice)."""
+        self._ok(self._L.esdg_set_element_variant(self.h, int(variant)))
 
     def state_pointers(self):
         """Device addresses (q, b, VdmInv) of the engine's own buffers."""

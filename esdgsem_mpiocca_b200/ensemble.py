@@ -107,6 +107,14 @@ class Ensemble:
         self._ok(self._L.esdg_ensemble_indicator_stats(self.h, out, int(reset)))
         return dict(zip(("net_zero", "net_full", "modal", "viscous"), [int(v) for v in out]))
 
+    def element_variants(self):
+        from .deviceclass import _element_variants
+        return _element_variants(self._L, self._L.esdg_ensemble_element_variants, self.h)
+
+    def set_element_variant(self, variant: int):
+        """Fixes the element-kernel variant (-1: the autotuner's choice)."""
+        self._ok(self._L.esdg_ensemble_set_element_variant(self.h, int(variant)))
+
     def set_stream(self, stream_ptr):
         self._ok(self._L.esdg_ensemble_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
 

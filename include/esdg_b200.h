@@ -154,13 +154,33 @@ int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES, double g_
 
 /* Element-kernel variant chosen by the engine's autotuner (no counterpart
  * in the reference): before the first step graph is captured the engine
- * times each compiled variant of the element kernel -- CTAs per SM the
- * register budget is cut for (2 or 3) and bulk-copy pipeline depth (2 or 3
- * tiles) -- on the mesh (writing only Qt) and keeps the fastest.
+ * times each compiled variant of the element kernel on the mesh (in the
+ * step's own update mode, on copies of q and gRK, each launch after an
+ * L2-sized flush) and keeps the fastest.  Variants 0-2: one thread per node
+ * (CTAs per SM the register budget is cut for, 2 or 3; bulk-copy pipeline
+ * depth, 2 or 3 tiles); variants 3-4 (N = 2..5): one thread per element row
+ * and column, each symmetric two-point flux evaluated once (two tile sizes).
  * *ctas_per_sm and *stages receive the choice (0: the one-shot kernel is
- * used), ms_variants3 [3] (may be NULL) the measured launch times.
+ * used), ms_variants3 [3] (may be NULL) the measured launch times of
+ * variants 0-2 (esdg_element_variants reports all of them).
  * ESDG_E_ARG before the tuning ran. */
 int esdg_tuned_config(const esdg_deviceclass* d, int* ctas_per_sm, int* stages, float* ms_variants3);
+
+/* All element-kernel variants (no counterpart in the reference): *count
+ * the number compiled, *chosen the one the steps use (-1: the one-shot
+ * kernel), and for the first cap of them ms [cap] the autotuner's launch
+ * times (0: not timed) and ctas_per_sm [cap] the resident CTAs per SM
+ * (0: not available for this degree / element count).  Pointers may be
+ * NULL.  ESDG_E_ARG before the tuning ran (or a variant was fixed). */
+int esdg_element_variants(const esdg_deviceclass* d, int* chosen, int* count, float* ms, int* ctas_per_sm,
+                          int cap);
+
+/* Fixes the element-kernel variant for every later step and RHS (no
+ * counterpart in the reference); -1 returns to the autotuner's choice.
+ * Call after buildDeviceKernels; re-captures the step graph if there is one.
+ * ESDG_E_UNSUPPORTED for a variant that is not available here.  All
+ * variants compute the same bits. */
+int esdg_set_element_variant(esdg_deviceclass* d, int variant);
 
 /* Device addresses of the solution q [K][3][(N+1)^2], the bathymetry b
  * [K][(N+1)^2] and VdmInv [(N+1)^2] owned by the engine (no counterpart in
@@ -255,6 +275,11 @@ int esdg_ensemble_set_stream(esdg_ensemble* en, void* cuda_stream);
  * ensemble (re-captures the step graph). */
 int esdg_ensemble_set_indicator(esdg_ensemble* en, int mode, const float* params, int nparams, float margin);
 int esdg_ensemble_indicator_stats(esdg_ensemble* en, unsigned long long* counts4, int reset);
+/* esdg_set_element_variant / esdg_element_variants for the ensemble's
+ * element kernel (no counterpart in the reference). */
+int esdg_ensemble_set_element_variant(esdg_ensemble* en, int variant);
+int esdg_ensemble_element_variants(const esdg_ensemble* en, int* chosen, int* count, float* ms, int* ctas_per_sm,
+                                   int cap);
 const char* esdg_ensemble_last_error(const esdg_ensemble* en);
 int esdg_ensemble_destroy(esdg_ensemble* en);
 
