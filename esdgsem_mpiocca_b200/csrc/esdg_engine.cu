@@ -134,7 +134,9 @@ class Engine {
     // Troubled-cell indicator of the artificial-viscosity path: 0 the modal
     // sensor and the viscous terms on every element (the reference's path);
     // 1 the modal sensor with the active set (viscous terms only on flagged
-    // elements, same numbers); 2 the learned indicator with the active set.
+    // elements, same numbers); 2 the learned indicator with the active set
+    // (one fused pass where the degree allows, N = 3); 3 the same decisions
+    // by three passes (features, network, sensor) at every degree.
     int indicator = 0;
     float* mlpP = nullptr;
     __nv_bfloat16* mlpPb = nullptr;
@@ -153,7 +155,7 @@ class Engine {
     std::vector<double> Vinv_h;
     std::vector<double> Dfd_h;  // flux-differencing matrix (host copy, row kernel parameter)
     int list_grid = 0;                        // persistent grid of the list kernels
-    int ind_grid[2] = {1, 1};                 // persistent grids of the indicator (modal, learned)
+    int ind_grid[3] = {1, 1, 1};              // persistent grids of the indicator (modal, learned, fused)
 
     // step graph
     cudaGraphExec_t graph = nullptr;
@@ -654,7 +656,13 @@ class Engine {
         ia.X = indX; ia.seta = ind_seta; ia.energy = ind_energy; ia.ok = ind_ok; ia.y = ind_y;
         using S = IndShape<NGL>;
         const int ntiles = (K + S::NE - 1) / S::NE;
-        if (indicator == 2) {
+        if (indicator == 2 && FusedShape<NGL>::OK) {
+            if constexpr (FusedShape<NGL>::OK) {
+                // features, network and sensor fallback in one pass
+                k_indicator_fused<NGL><<<std::min(ntiles, ind_grid[2]), S::THREADS, 0, stream>>>(ia, ntiles);
+                ++launches;
+            }
+        } else if (indicator >= 2) {
             if constexpr (NGL >= 4 && NGL <= 6) {
                 // the network as one batched GEMM over the elements:
                 // features, forward pass, then the sensor where unsure
@@ -690,6 +698,12 @@ class Engine {
         if (e != cudaSuccess) return cuda_fail(e, "occupancy (indicator)");
         ind_grid[0] = std::max(1, o0) * sms;
         ind_grid[1] = std::max(1, o1) * sms;
+        if constexpr (FusedShape<NGL>::OK) {
+            int o2 = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_indicator_fused<NGL>, FusedShape<NGL>::THREADS, 0);
+            if (e != cudaSuccess) return cuda_fail(e, "occupancy (fused indicator)");
+            ind_grid[2] = std::max(1, o2) * sms;
+        }
         if constexpr (NGL >= 4 && NGL <= 6) {
             constexpr int KP = mlp_kp(NGL);
             e = cudaFuncSetAttribute(k_mlp_forward<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -704,13 +718,13 @@ class Engine {
         return 0;
     }
 
-    // Selects the indicator (0, 1, 2; see `indicator`); P (mode 2) is the
+    // Selects the indicator (0..3; see `indicator`); P (modes 2, 3) is the
     // network's FP32 parameter block of mlp_layout(ngl).total floats.
     int set_indicator(int mode, const float* P_h, int nP, float margin) {
         if (!inited || !built) return fail(ESDG_E_ARG, "set_indicator after buildDeviceKernels");
-        if (mode < 0 || mode > 2) return fail(ESDG_E_ARG, "indicator mode must be 0, 1 or 2");
+        if (mode < 0 || mode > 3) return fail(ESDG_E_ARG, "indicator mode must be 0, 1, 2 or 3");
         if (mode > 0 && !AV) return fail(ESDG_E_ARG, "the indicator needs ArtificialViscosity=1");
-        if (mode == 2) {
+        if (mode >= 2) {
             if (ngl < 4 || ngl > 6) return fail(ESDG_E_UNSUPPORTED, "the learned indicator supports N = 3..5");
             if (!P_h || nP != mlp_layout(ngl).total)
                 return fail(ESDG_E_ARG, "learned indicator: parameter block of " +
@@ -727,7 +741,7 @@ class Engine {
             if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
             k_build_nbr<<<(K + 255) / 256, 256, 0, stream>>>(0, K, side, ftab, nbr);
         }
-        if (mode == 2) {
+        if (mode >= 2) {
             const int n = mlp_layout(ngl).total;
             if (!mlpP) {
                 if ((r = alloc(&mlpP, (size_t)n)) || (r = alloc(&mlpPb, (size_t)n)) ||

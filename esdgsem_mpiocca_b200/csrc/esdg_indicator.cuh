@@ -406,4 +406,180 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
     }
 }
 
+// The learned indicator in one pass, for degrees whose element is an
+// aligned lane group (n^2 divides 32) and whose tile of NE elements fills
+// whole 16-row MMA tiles: per tile the features of k_ind_features (same
+// arithmetic, same shuffle order) go to a BF16 tile in shared memory, the
+// first NE/16 warps run mlp_warp_forward_regs on it (the arithmetic of
+// k_mlp_forward), and the decision and modal fallback of k_indicator<NGL,
+// true> follow.  The modal transform of an element involves only its own
+// lane group, so it runs per warp (warp barriers) and only in warps that
+// hold an element the network leaves to the sensor.  q and b are read once
+// per stage instead of three passes over q, features and outputs.
+template <int NGL>
+struct FusedShape {
+    static constexpr int N2 = NGL * NGL, NE = IndShape<NGL>::NE, THREADS = IndShape<NGL>::THREADS;
+    static constexpr int KP = mlp_kp(NGL);
+    static constexpr int MT = NE / 16;  // MMA row tiles per element tile
+    static constexpr bool OK = (32 % N2) == 0 && NE % 16 == 0 && MT <= THREADS / 32 && NGL >= 4 && NGL <= 6;
+};
+
+template <int NGL>
+__global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused(IndArgs a, int ntiles) {
+    using S = FusedShape<NGL>;
+    constexpr int N2 = S::N2, NE = S::NE, KP = S::KP;
+    static_assert(S::OK, "fused indicator: element = aligned lane group, whole 16-row tiles");
+    if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
+    __shared__ __align__(16) __nv_bfloat16 sW1[MLP_H * KP];
+    __shared__ __align__(16) __nv_bfloat16 sW2[MLP_H * MLP_H];
+    __shared__ __align__(16) __nv_bfloat16 sX[NE * KP];
+    __shared__ float sy[NE], sseta[NE];
+    __shared__ double sV[N2];
+    __shared__ double seta[NE * N2], sM[NE * N2], sW[NE * N2];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int el = tid / N2, nd = tid % N2;
+    const int s = el * N2 + nd;
+    if (tid < N2) sV[tid] = a.Vinv[tid];
+    mlp_stage_weights(KP, a.Pb, a.L, sW1, sW2);
+    MlpLaneParams R{};
+    if (warp < S::MT) R = mlp_lane_params(a.P, a.L);
+    __syncthreads();
+    struct Ld {
+        double h, b, hu, hv;
+        int ins;
+        int4 nb;
+    };
+    auto fetch = [&](int t) {
+        Ld L{1.0, 0.0, 0.0, 0.0, -1, make_int4(-1, -1, -1, -1)};
+        const int e = t * NE + el;
+        if (e < a.K) {
+            const long qid = (long)e * 3 * N2 + nd;
+            L.h = a.q[qid];
+            L.b = a.B[(long)e * N2 + nd];
+            L.hu = a.q[qid + N2];
+            L.hv = a.q[qid + 2 * N2];
+            L.ins = inst_of(a.elem_inst, e);
+            if (nd == 0 && a.act) L.nb = a.nbr[e];
+        }
+        return L;
+    };
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    int t = blockIdx.x;
+    Ld nxt = (t < ntiles) ? fetch(t) : Ld{1.0, 0.0, 0.0, 0.0, -1, make_int4(-1, -1, -1, -1)};
+    for (; t < ntiles; t += gridDim.x) {
+        const Ld cur = nxt;
+        if (t + gridDim.x < ntiles) nxt = fetch(t + gridDim.x);
+        const int e = t * NE + el;
+        const bool live = e < a.K && !a.st[cur.ins].done;
+        // ---- features (k_ind_features) ----
+        const double v3[3] = {cur.b + cur.h, cur.hu, cur.hv};
+        seta[s] = v3[0];
+        double mh = cur.h, e2 = v3[0] * v3[0];
+        bool fin = isfinite(cur.h) && isfinite(cur.hu) && isfinite(cur.hv);
+        double m3[3] = {v3[0], v3[1], v3[2]};
+#pragma unroll
+        for (int off = N2 / 2; off > 0; off >>= 1) {
+#pragma unroll
+            for (int f = 0; f < 3; ++f) m3[f] += __shfl_xor_sync(0xffffffffu, m3[f], off);
+            mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
+            e2 += __shfl_xor_sync(0xffffffffu, e2, off);
+            fin = __shfl_xor_sync(0xffffffffu, (int)fin, off) && fin;
+        }
+        float dv[3], d3f[3];
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            m3[f] /= N2;
+            dv[f] = (float)(v3[f] - m3[f]);
+            d3f[f] = dv[f] * dv[f];
+        }
+#pragma unroll
+        for (int off = N2 / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int f = 0; f < 3; ++f) d3f[f] += __shfl_xor_sync(0xffffffffu, d3f[f], off);
+        __nv_bfloat16* xr = sX + el * KP;
+        float rmsf[3];
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            rmsf[f] = sqrtf(d3f[f] * (1.0f / N2));
+            const float mf = fabsf((float)m3[f]);
+            const float inv = (rmsf[f] > (float)MLP_REL_FLAT * mf && rmsf[f] > 0.0f) ? 1.0f / rmsf[f] : 0.0f;
+            xr[f * N2 + nd] = __float2bfloat16(dv[f] * inv);
+        }
+        if (nd < 3) {  // lanes 0, 1, 2 of the group: the scale feature of their field
+            const float r = nd == 0 ? rmsf[0] : (nd == 1 ? rmsf[1] : rmsf[2]);
+            const float m = (float)(nd == 0 ? m3[0] : (nd == 1 ? m3[1] : m3[2]));
+            const float tot = m * m + r * r;
+            const float sf = (tot > 0.0f && r > 0.0f) ? fmaxf(log10f(r * r / tot), (float)MLP_S_MIN) : (float)MLP_S_MIN;
+            xr[3 * N2 + nd] = __float2bfloat16(0.25f * sf);
+            if (nd == 0) sseta[el] = sf;
+        }
+        for (int c = 3 * N2 + 3 + nd; c < KP; c += N2) xr[c] = __float2bfloat16(0.0f);
+        const int ok = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
+        __syncthreads();  // feature tile complete
+        // ---- network (k_mlp_forward) ----
+        if (warp < S::MT) {
+            float ylo, yhi;
+            mlp_warp_forward_regs<KP>(sX + warp * 16 * KP, sW1, sW2, R, ylo, yhi);
+            if ((lane & 3) == 0) {
+                sy[warp * 16 + (lane >> 2)] = ylo;
+                sy[warp * 16 + (lane >> 2) + 8] = yhi;
+            }
+        }
+        __syncthreads();  // outputs complete; the feature tile may be rewritten after this
+        // ---- decision and modal fallback (k_indicator<NGL, true>), per lane group ----
+        int nm = 1, vd = 0;
+        if (live) {
+            const double sig = (double)sy[el] + (double)sseta[el];
+            nm = learned_needs_modal(a, sig, e2, ok);
+            vd = (nm == 0 && a.emax * e2 >= a.c.ZeroTOL && sig > a.c.sigmaMax + a.margin) ? 1 : 0;
+        }
+        bool clear = false;
+        if (__any_sync(0xffffffffu, live && nm)) {
+            const int i = nd / NGL, j = nd % NGL;  // entry (i, j) of M1 and w
+            sM[s] = sensor_m1<NGL>(sV, seta + el * N2, i, j);
+            __syncwarp();
+            sW[s] = sensor_w<NGL>(sV, sM + el * N2, i, j);
+            __syncwarp();
+            const double w = sW[s], w2 = w * w;
+            constexpr int N = NGL - 1;
+            double z1 = ((i == N) || (j == N)) ? w2 : 0.0;
+            double z2 = (((i == N - 1) && (j <= N - 1)) || ((j == N - 1) && (i <= N - 1))) ? w2 : 0.0;
+            double n1 = w2;
+            double n2 = (i < N && j < N) ? w2 : 0.0;
+#pragma unroll
+            for (int off = N2 / 2; off > 0; off >>= 1) {
+                z1 += __shfl_xor_sync(0xffffffffu, z1, off);
+                z2 += __shfl_xor_sync(0xffffffffu, z2, off);
+                n1 += __shfl_xor_sync(0xffffffffu, n1, off);
+                n2 += __shfl_xor_sync(0xffffffffu, n2, off);
+            }
+            const double thr = a.c.sensor_skip * (1.0 - 1e-6);
+            clear = n1 > a.c.ZeroTOL * (1.0 + 1e-6) && z1 < thr * n1 && z2 < thr * n2;
+            clear = clear || (n1 < a.c.ZeroTOL * (1.0 - 1e-6));
+        }
+        if (live && nd == 0) {
+            double v = 0.0;
+            int kind = 2;  // 0 net zero, 1 net eps0, 2 modal
+            if (nm) {
+                v = clear ? 0.0 : sensor_tail<NGL>(a.c, sW + el * N2);
+            } else {
+                kind = vd;
+                v = kind ? a.c.eps0 : 0.0;
+            }
+            a.VP[e] = v;
+            if (a.stage0 && v > 0.0) atomicMax(&a.st[cur.ins].visc_key, dbl_key(v));
+            if (a.act && !(v <= 0.0)) mark_active(a.act, e, cur.nb);
+            cnt[kind] += 1;
+            if (!(v <= 0.0)) cnt[3] += 1;
+        }
+        __syncwarp();  // the group's shared rows are rewritten next tile
+    }
+    if (a.stats) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (cnt[k]) atomicAdd(&a.stats[k], cnt[k]);
+    }
+}
+
 }  // namespace esdg

@@ -151,7 +151,7 @@ class DeviceClass:
         the viscous terms everywhere (the reference's path), 1 the modal
         sensor with the active set, 2 the learned indicator (`net`, an
         indicator.IndicatorNet) with the active set."""
-        P, n, margin = _indicator_params(net) if mode == 2 else (None, 0, 0.0)
+        P, n, margin = _indicator_params(net) if mode >= 2 else (None, 0, 0.0)
         self._ok(self._L.esdg_set_indicator(self.h, mode, P, n, margin))
 
     def indicator_stats(self, reset: bool = False):

@@ -99,7 +99,7 @@ class Ensemble:
         path); 1: modal sensor with the active set; 2: the learned indicator
         (indicator.IndicatorNet) with the active set."""
         from .deviceclass import _indicator_params
-        P, n, margin = _indicator_params(net) if mode == 2 else (None, 0, 0.0)
+        P, n, margin = _indicator_params(net) if mode >= 2 else (None, 0, 0.0)
         self._ok(self._L.esdg_ensemble_set_indicator(self.h, mode, P, n, margin))
 
     def indicator_stats(self, reset: bool = False):

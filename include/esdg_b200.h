@@ -204,7 +204,11 @@ int esdg_state_pointers(esdg_deviceclass* d, const double** q, const double** b,
  *           sigma < sigma_min - margin and eps0 where it predicts
  *           sigma > sigma_max + margin; the modal sensor decides every other
  *           element (the ramp band, positivity check failures, modal energy
- *           near ZeroTOL).  N in 3..5.
+ *           near ZeroTOL).  N in 3..5.  At N = 3 features, network and
+ *           sensor fallback run as one fused pass over the state;
+ *   mode 3  mode 2's decisions computed by three separate passes (feature
+ *           rows, batched network, sensor) at every degree; the same
+ *           numbers as mode 2.
  * params/nparams/margin are ignored for modes 0 and 1. */
 int esdg_set_indicator(esdg_deviceclass* d, int mode, const float* params, int nparams, float margin);
 

@@ -104,3 +104,39 @@ def test_indicator_needs_artificial_viscosity():
     prob = problems.periodic_bump(steps=2)
     with pytest.raises(EsdgError):
         Solver(prob, indicator=1)
+
+
+@pytest.mark.parametrize("make", [
+    lambda: problems.tsunami_member(11, sizes=(64,)),
+    lambda: problems.dam_break(N=3, nel=32, seed=5),
+])
+def test_fused_learned_pass_equals_three_passes(make):
+    """Mode 2 at N = 3 runs features, network and sensor fallback as one
+    fused kernel; mode 3 runs the three separate passes.  Same decisions,
+    same solution, bit for bit."""
+    prob = make()
+    net = IndicatorNet.default(3)
+    q2, st2 = _run(prob, 30, 2, net)
+    q3, st3 = _run(prob, 30, 3, net)
+    np.testing.assert_array_equal(q2, q3)
+    assert st2 == st3
+    assert st2["net_zero"] + st2["net_full"] > 0
+
+
+def test_fused_learned_pass_in_the_arena():
+    from esdgsem_mpiocca_b200.ensemble import Ensemble
+    probs = [problems.tsunami_member(s, sizes=(32,)) for s in (21, 22, 23)]
+    steps = [25, 15, 20]
+    out = {}
+    for mode in (2, 3):
+        ens = Ensemble.for_problems(probs)
+        try:
+            ens.set_indicator(mode, IndicatorNet.default(3))
+            ids = [ens.add(p, T=1e9, max_steps=s) for p, s in zip(probs, steps)]
+            ens.run_until_done(ids)
+            out[mode] = ([ens.q(i) for i in ids], ens.indicator_stats())
+        finally:
+            ens.close()
+    for a, b in zip(out[2][0], out[3][0]):
+        np.testing.assert_array_equal(a, b)
+    assert out[2][1] == out[3][1]
