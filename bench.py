@@ -157,9 +157,11 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per k_element launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_element_curved_lake_512_N4.md")
+def profiled_traffic(kernel=""):
+    """DRAM bytes per launch of the element kernel in use, from the
+    committed ncu summary of that kernel."""
+    name = "k_element_rows" if kernel.startswith("k_element_rows") else "k_element"
+    p = os.path.join(ROOT, "profiles", f"{name}_curved_lake_512_N4.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -274,7 +276,7 @@ def main():
 
     hbm, peak_kind = peaks()
     ach = ELEM_BYTES_PER_NODE * prob.dofs() / (kern["ms"] / 1e3) / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(element_kernel_name(s.dc))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
