@@ -109,11 +109,13 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
     if (a.extent && f >= a.extent[1]) return;
     constexpr int N2 = NGL * NGL;
     const int4 t = a.ftab[f];
+    // the face's own data does not depend on the table entry: requested
+    // together with it, ahead of the instance check
+    const long ex = (long)f * NGL + i;
+    const double nx = a.nx[ex], ny = a.ny[ex], sc = a.scal[ex], bLx = a.bL[ex];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
     if (a.st[inst_of(a.elem_inst, eL)].done) return;
     const int ir = same ? i : NGL - 1 - i;
-    const long ex = (long)f * NGL + i;
-    const double nx = a.nx[ex], ny = a.ny[ex];
     const double* qe = a.q + (long)eL * 3 * N2;
     const int oL = trace_offset(sL, i, NGL);
     const double hL = qe[oL], huL = qe[oL + N2], hvL = qe[oL + 2 * N2];
@@ -137,8 +139,8 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
         if (grad) { ghR = hL; ghuR = huL; ghvR = hvL; }
     }
     double N0, N1, N2f;
-    es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, a.bL[ex], a.bR[(long)f * NGL + ir], N0, N1, N2f);
-    const double s = a.scal[ex];
+    es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, bLx, a.bR[(long)f * NGL + ir], N0, N1, N2f);
+    const double s = sc;
     double* sp = a.SP + (long)f * 3 * NGL + i;
     sp[0] = s * a.c.geomFace * N0;
     sp[NGL] = s * a.c.geomFace * N1;
