@@ -46,6 +46,8 @@ def _declare(lib):
         "esdg_profile_steps": (_I, [_VP, _I, _PD, _PD]),
         "esdg_compute_rhs_noalloc": (_I, [_I, _I, _I, _I, _I, _D, _D] + [_VP] * 17 + [_VP, _VP]),
         "esdg_basis": (_I, [_I, _I] + [_PD] * 9),
+        "esdg_basis_fd": (_I, [_I, _PD, _PD, _PD]),
+        "esdg_copy_partial_dry_data": (_I, [_VP, _PD, _PD, _PD]),
         "esdg_mesh_cartesian": (_I, [_I, _D, _D, _D, _D, _I, _I, _I, _I, ctypes.POINTER(_VP)]),
         "esdg_mesh_mapped": (_I, [_I, _D, _D, _D, _D, _I, _I, _D, _I, ctypes.c_uint, ctypes.POINTER(_VP)]),
         "esdg_mesh_read_ism2": (_I, [_I, ctypes.c_char_p, _I, _I, ctypes.POINTER(_VP)]),

@@ -154,6 +154,10 @@ class Engine {
     unsigned long long* ind_stats = nullptr;  // [4] decision counts
     std::vector<double> Vinv_h;
     std::vector<double> Dfd_h;  // flux-differencing matrix (host copy, row kernel parameter)
+    // partial-dry treatment: per-element dry flag, difference matrices
+    int* dry = nullptr;
+    double *DcFD = nullptr, *DupFD = nullptr, *DdnFD = nullptr;
+    bool pd_copied = false;
     int list_grid = 0;                        // persistent grid of the list kernels
     int ind_grid[3] = {1, 1, 1};              // persistent grids of the indicator (modal, learned, fused)
 
@@ -199,6 +203,7 @@ class Engine {
         mlpP = nullptr; mlpPb = nullptr; act = alist = nullptr; ind_stats = nullptr; nbr = nullptr; extent = nullptr;
         indX = nullptr; ind_seta = ind_y = nullptr; ind_energy = nullptr; ind_ok = nullptr;
         indicator = 0;
+        dry = nullptr; DcFD = DupFD = DdnFD = nullptr; pd_copied = false;
         inited = copied = built = false;
     }
 
@@ -227,7 +232,6 @@ class Engine {
         if ((long long)K_ * (N_ + 1) * (N_ + 1) * 3 > (1ll << 31) - 1)
             return fail(ESDG_E_ARG, "Nelem*3*(N+1)^2 must fit a 32-bit int (as in the reference)");
         if (DiscBottom_) return fail(ESDG_E_UNSUPPORTED, "DiscBottom=1 is outside the rebuilt hot path");
-        if (PartialDry_) return fail(ESDG_E_UNSUPPORTED, "PartialDryTreatment=1 is outside the rebuilt hot path");
         if (Friction_) return fail(ESDG_E_UNSUPPORTED, "FrictionTerms=1 is outside the rebuilt hot path");
         N = N_; ngl = N + 1; K = K_; F = F_; rank = rank_; rkSSP = rkSSP_; ES = ES_; Testcase = Testcase_;
         eps0 = eps0_; sigma_max = smax; sigma_min = smin; PosPresTOL = tol; geomFace = geomface; g = g_;
@@ -248,6 +252,11 @@ class Engine {
             return r;
         if ((r = alloc(&EdgeData, (size_t)F * 8)) || (r = alloc(&ftab, (size_t)F)) || (r = alloc(&side, (size_t)K * 4)))
             return r;
+        if (PartialDry) {
+            if ((r = alloc(&dry, (size_t)K)) || (r = alloc(&DcFD, n2)) || (r = alloc(&DupFD, n2)) ||
+                (r = alloc(&DdnFD, n2)))
+                return r;
+        }
         if (AV) {
             if ((r = alloc(&SGX, nf * 2)) || (r = alloc(&SGY, nf * 2)) || (r = alloc(&SPV, nf * 2)) ||
                 (r = alloc(&GX, nn * 2)) || (r = alloc(&GY, nn * 2)) || (r = alloc(&VP, (size_t)K)))
@@ -404,6 +413,9 @@ class Engine {
         a.SPV = SPV; a.side = side; a.q = q; a.gRK = gRK; a.Qt = Qt; a.Qtmp = Qtmp; a.GX = GX; a.GY = GY; a.VP = VP;
         a.elem_inst = elem_inst; a.st = st; a.rkA = A; a.rkB = Bc; a.rkC = C; a.mode = mode; a.lam = lam;
         a.c = phys(); a.extent = extent;
+        if (PartialDry) {
+            a.dry = dry; a.Bn = B; a.Dc = DcFD; a.Dup = DupFD; a.Ddn = DdnFD;
+        }
         return a;
     }
 
@@ -598,6 +610,7 @@ class Engine {
         using S = ElemShape<NGL>;
         const int eb = (K + S::NE - 1) / S::NE;
         const int lam_in_elem = (last && !PP) ? 1 : 0;
+        launch_find_dry<NGL>();
         if (AV && indicator) {
             // active set: indicator (stages > 0; stage 0's runs before the
             // step's dt), plain element kernel (flagged elements only write
@@ -817,7 +830,32 @@ class Engine {
 
     int check_ready() {
         if (!inited || !copied || !built) return fail(ESDG_E_ARG, "call initDeviceVariables, copyDeviceVariables and buildDeviceKernels first");
+        if (PartialDry && !pd_copied) return fail(ESDG_E_ARG, "PartialDryTreatment=1: call copyPartialDryData first");
         return 0;
+    }
+
+    // deviceclass::copyPartialDryData (src/deviceclass.cpp:546-553).
+    int copy_partial_dry(const double* Dc, const double* Df, const double* Db) {
+        if (!inited) return fail(ESDG_E_ARG, "copyPartialDryData before initDeviceVariables");
+        if (!PartialDry) return fail(ESDG_E_ARG, "copyPartialDryData needs PartialDryTreatment=1 at initDeviceVariables");
+        if (!Dc || !Df || !Db) return fail(ESDG_E_ARG, "null difference matrix");
+        const size_t n2 = (size_t)ngl * ngl;
+        int r = 0;
+        if ((r = h2d(DcFD, Dc, n2, "DCentralFD")) || (r = h2d(DupFD, Df, n2, "DforwardFD")) ||
+            (r = h2d(DdnFD, Db, n2, "DbackwardFD")))
+            return r;
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copyPartialDryData");
+        pd_copied = true;
+        return 0;
+    }
+
+    // FindDryElements of the stage (okl/PartialDryTreatment/FindDryElements.okl).
+    template <int NGL>
+    void launch_find_dry() {
+        if (!PartialDry) return;
+        k_find_dry<NGL><<<(K + 255) / 256, 256, 0, stream>>>(K, q, dry, PosPresTOL);
+        ++launches;
     }
 
     // Fixes the element-kernel variant (-1: let the autotuner pick).
@@ -969,6 +1007,7 @@ class Engine {
             const bool last = s == gStages - 1;
             const int mode = rkSSP ? 1 : 0;
             const int lam_in_elem = (last && !PP) ? 1 : 0;
+            launch_find_dry<NGL>();
             cudaEventRecord(pev[0], stream);
             launch_face<NGL>(AV != 0);
             cudaEventRecord(pev[1], stream);
@@ -1145,6 +1184,12 @@ int esdg_copy_device_variables(esdg_deviceclass* d, int PositivityPreserving, in
                        ElemEdgeMasterSlave, ElemEdgeOrientation, ElemToEdge, EdgeData, EdgeReversed);
 }
 
+int esdg_copy_partial_dry_data(esdg_deviceclass* d, const double* DCentralFD, const double* DforwardFD,
+                               const double* DbackwardFD) {
+    ESDG_GUARD(d);
+    return d->eng.copy_partial_dry(DCentralFD, DforwardFD, DbackwardFD);
+}
+
 int esdg_build_device_kernels(esdg_deviceclass* d, int KernelVersion, int KernelVersionSTD, int Testcase,
                               int FluxDifferencing, int NumFlux, int rkSSP, int ArtificialViscosity,
                               int PositivityPreserving, int DiscBottom) {
@@ -1313,6 +1358,38 @@ int esdg_advance(esdg_deviceclass* d, int nsteps, double T, double* t_out, int* 
 // ---------------------------------------------------------------------------
 // Set-up
 // ---------------------------------------------------------------------------
+int esdg_basis_fd(int N, double* Dc, double* Df, double* Db) {
+    // src/basis.cpp:190-229: two-point differences on the LGL nodes; row i of
+    // each matrix holds the weights of node i's difference (all other
+    // entries zero).  Central: one-sided at the two ends.
+    if (N < 1 || N > 15 || !Dc || !Df || !Db) return ESDG_E_ARG;
+    std::vector<double> x(N + 1), w(N + 1);
+    esdg::lgl_nodes_weights(N, x.data(), w.data());
+    const int n = N + 1, n2 = n * n;
+    for (int k = 0; k < n2; ++k) Dc[k] = Df[k] = Db[k] = 0.0;
+    const double first = 1.0 / (x[1] - x[0]), last = 1.0 / (x[N] - x[N - 1]);
+    Dc[0] = -first; Dc[1] = first;
+    Dc[n2 - 2] = -last; Dc[n2 - 1] = last;
+    for (int i = 1; i + 1 < n; ++i) {
+        const double c = 1.0 / (x[i + 1] - x[i - 1]);
+        Dc[i * n + i - 1] = -c;
+        Dc[i * n + i + 1] = c;
+    }
+    for (int i = 0; i + 1 < n; ++i) {  // forward: node i and i+1
+        const double c = 1.0 / (x[i + 1] - x[i]);
+        Df[i * n + i] = -c;
+        Df[i * n + i + 1] = c;
+    }
+    Df[n2 - 2] = -last; Df[n2 - 1] = last;  // last row: backward
+    Db[0] = -first; Db[1] = first;          // first row: forward
+    for (int i = 1; i < n; ++i) {  // backward: node i-1 and i
+        const double c = 1.0 / (x[i] - x[i - 1]);
+        Db[i * n + i - 1] = -c;
+        Db[i * n + i] = c;
+    }
+    return ESDG_OK;
+}
+
 int esdg_basis(int N, int FluxDifferencing, double* xGL, double* wGL, double* xG, double* wG, double* D, double* D0,
                double* Dstrong, double* Dhat, double* VdmInv) {
     if (N < 1 || N > 15) return ESDG_E_ARG;

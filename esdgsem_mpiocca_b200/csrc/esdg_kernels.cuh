@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include "esdg_physics.cuh"
+#include "esdg_partialdry.cuh"
 
 namespace esdg {
 
@@ -94,6 +95,13 @@ struct ElemArgs {
     int* alist = nullptr;
     int* acount = nullptr;
     const int* __restrict__ extent = nullptr;  // live extent, as in FaceArgs
+    // Partial-dry treatment (null: off): per-element dry flag, nodal b, and
+    // the central / forward / backward difference matrices [n*n].
+    const int* __restrict__ dry = nullptr;
+    const double* __restrict__ Bn = nullptr;
+    const double* __restrict__ Dc = nullptr;
+    const double* __restrict__ Dup = nullptr;
+    const double* __restrict__ Ddn = nullptr;
 };
 
 __device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return elem_inst ? elem_inst[e] : 0; }
@@ -337,6 +345,9 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
         double r0 = -J * d1;
         double r1 = -J * d2 - a.c.g * h * bx;
         double r2 = -J * d3 - a.c.g * h * by;
+        if (a.dry && a.dry[e])
+            pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sh + el * N2, a.Bn + (long)e * N2, eta, xi, ye, yx, xe, xx, J, r1,
+                           r2);
         // lift: sides 0/2 first, then 1/3 (DBSurf1/2 are zero)
         const double db = 0.0;
 #pragma unroll
@@ -484,6 +495,9 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av1(ElemArg
         double r0 = -J * d1;
         double r1 = -J * d2 - a.c.g * h * a.Bx[xid];
         double r2 = -J * d3 - a.c.g * h * a.By[xid];
+        if (a.dry && a.dry[e])
+            pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sh + el * N2, a.Bn + (long)e * N2, eta, xi, ye, yx, xe, xx, J, r1,
+                           r2);
         double gx0 = 0, gx1 = 0, gy0 = 0, gy1 = 0;
         {
             // calcGradient: u_xi = sum_l Dhat[xi][l] u(l,eta), u_eta = sum_l Dhat[eta][l] u(xi,l)

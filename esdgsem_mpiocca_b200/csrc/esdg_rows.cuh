@@ -18,11 +18,12 @@
 // Qtmp, Jinv, Bx, By, Y_xi, Y_eta, X_xi, X_eta, the side table) into the
 // stage's buffer; the updated q (and gRK) are written back into the same
 // buffer and leave with one bulk store per array when every element of the
-// tile is active, by plain stores otherwise.  Thread t works on element
-// t % NE, line t / NE: consecutive threads touch consecutive elements, whose
-// shared-memory slots lie an odd number of doubles apart (3 N2 or N2 with
-// N2 odd, or a multiple of 16 bytes apart with an odd quotient), so the
-// accesses of a half-warp fall in distinct banks.
+// tile is active and none is partly dry, by plain stores otherwise.  Thread
+// t works on element t % NE, line t / NE: consecutive threads touch
+// consecutive elements, whose shared-memory slots lie an odd number of
+// doubles apart (3 N2 or N2 with N2 odd, or a multiple of 16 bytes apart
+// with an odd quotient), so the accesses of a half-warp fall in distinct
+// banks.
 #pragma once
 
 #include "esdg_tma.cuh"
@@ -235,7 +236,9 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
         }
         // every element of the tile active: the update goes back through the
         // stage buffer and one bulk store per array
-        const int idle = __syncthreads_or(inb && !active);  // also the barrier between the two sums
+        // also the barrier between the two sums; a partly dry element reads
+        // its neighbours' old h in the update, so such tiles store directly
+        const int idle = __syncthreads_or((inb && !active) || (active && a.dry && a.dry[e]));
         const bool bulk = (a.mode != 2) && !idle;
         // ---- eta sums, surface lift and update: column ln of element el ----
         double lam = 0.0;
@@ -289,6 +292,9 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
                 double r0 = -J * e1;
                 double r1 = -J * e2 - a.c.g * h[j] * sBx[s];
                 double r2 = -J * e3 - a.c.g * h[j] * sBy[s];
+                if (a.dry && a.dry[e])
+                    pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sq + el * 3 * N2, a.Bn + (long)e * N2, j, ln, sYe[s],
+                                   sYx[s], sXe[s], sXx[s], J, r1, r2);
                 const double db = 0.0;
                 if (j == 0 || j == NGL - 1) {  // eta sides (0 at j = 0, 2 at j = NGL-1)
                     const int m = (j == 0) ? a0.y : a2.y;

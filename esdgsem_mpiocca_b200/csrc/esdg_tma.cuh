@@ -271,6 +271,9 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
             double r0 = -J * d1;
             double r1 = -J * d2 - a.c.g * h * sBx[s];
             double r2 = -J * d3 - a.c.g * h * sBy[s];
+            if (a.dry && a.dry[e])
+                pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sq + el * 3 * N2, a.Bn + (long)e * N2, eta, xi, ye, yx, xe, xx,
+                               J, r1, r2);
             const double db = 0.0;
 #pragma unroll
             for (int pass = 0; pass < 2; ++pass) {

@@ -83,6 +83,12 @@ class DeviceClass:
         self._ok(self._L.esdg_copy_device_variables(self.h, PositivityPreserving, Nelem, *[pd(a) for a in d],
                                                     *[pi(a) for a in i]))
 
+    def copyPartialDryData(self, DCentralFD, DforwardFD, DbackwardFD):
+        """The difference matrices of the partial-dry volume term
+        (deviceclass::copyPartialDryData; host.Basis.fd())."""
+        d = [_f64(a) for a in (DCentralFD, DforwardFD, DbackwardFD)]
+        self._ok(self._L.esdg_copy_partial_dry_data(self.h, *[pd(a) for a in d]))
+
     def buildDeviceKernels(self, KernelVersion, KernelVersionSTD, Testcase, FluxDifferencing, NumFlux, rkSSP,
                            ArtificialViscosity, PositivityPreserving, DiscBottom):
         self._ok(self._L.esdg_build_device_kernels(self.h, KernelVersion, KernelVersionSTD, Testcase,
@@ -208,13 +214,15 @@ class Solver:
         self.dc = DeviceClass(0, device_id)
         self.dc.initDeviceVariables(p.N, m.K, m.F, 0, p.rkSSP, p.NEpad, p.NEsurfpad, p.Nedgepad, p.NavgPad, p.ES,
                                     p.Testcase, p.epsilon_0, p.sigma_max, p.sigma_min, p.PosPresTOL, bs.geomface,
-                                    p.g_const, p.PositivityPreserving, p.ArtificialViscosity, p.DiscBottom, 0.0, 0, 0,
-                                    0, 0, 0)
+                                    p.g_const, p.PositivityPreserving, p.ArtificialViscosity, p.DiscBottom, 0.0,
+                                    p.PartialDryTreatment, 0, 0, 0, 0)
         zeros = np.zeros_like(prob.q0)
         self.dc.copyDeviceVariables(p.PositivityPreserving, m.K, bs.wGL, m.nx, m.ny, m.scal, m.y_xi, m.y_eta, m.x_xi,
                                     m.x_eta, prob.b, prob.Bx, prob.By, bs.D, bs.Dstrong, bs.Dhat, m.Jinv, m.x, m.y,
                                     prob.q0 if q0 is None else q0, prob.EleSizes, zeros, zeros, bs.VdmInv,
                                     m.MasterSlave, m.Orientation, m.ElemToEdge, m.EdgeData, m.EdgeReversed)
+        if p.PartialDryTreatment:
+            self.dc.copyPartialDryData(*(getattr(bs, "fd_mats", None) or bs.fd()))
         self.dc.buildDeviceKernels(99, 99, p.Testcase, p.FluxDifferencing, p.NumFlux, p.rkSSP, p.ArtificialViscosity,
                                    p.PositivityPreserving, p.DiscBottom)
         if indicator:

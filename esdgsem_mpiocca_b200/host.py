@@ -54,6 +54,14 @@ class Basis:
         """1/w_0 (main.cpp:921)."""
         return 1.0 / self.wGL[0]
 
+    def fd(self):
+        """Central, forward and backward difference matrices [n*n] of the
+        partial-dry treatment (src/basis.cpp:190-229)."""
+        n2 = (self.N + 1) ** 2
+        out = [np.zeros(n2) for _ in range(3)]
+        _check(_lib().esdg_basis_fd(self.N, *[pd(a) for a in out]), "esdg_basis_fd")
+        return tuple(out)
+
 
 @dataclass
 class MeshArrays:
@@ -194,6 +202,7 @@ class Params:
     Nedgepad: int = 16
     NavgPad: int = 10
     DiscBottom: int = 0
+    PartialDryTreatment: int = 0
     MaxSteps: int = 0
 
 

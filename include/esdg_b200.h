@@ -59,6 +59,14 @@ int esdg_copy_device_variables(esdg_deviceclass* d, int PositivityPreserving, in
                                const int* ElemEdgeOrientation, const int* ElemToEdge, const int* EdgeData,
                                const int* EdgeReversed);
 
+/* deviceclass::copyPartialDryData -- include/deviceclass.h:69-71,
+ * src/deviceclass.cpp:546-553: the finite-difference matrices [n*n] of the
+ * partial-dry volume term (basis::FiniteDifferenceOperators, esdg_basis_fd).
+ * Only with PartialDry = 1 at esdg_init_device_variables; required before
+ * the first time step or RHS then. */
+int esdg_copy_partial_dry_data(esdg_deviceclass* d, const double* DCentralFD, const double* DforwardFD,
+                               const double* DbackwardFD);
+
 /* deviceclass::buildDeviceKernels -- include/deviceclass.h:60-68,
  * src/deviceclass.cpp:349-544 (kernel selection; here: choice among the
  * compiled sm_100a instantiations). */
@@ -336,6 +344,11 @@ typedef struct esdg_mesh esdg_mesh;
  * D0 (plain collocation derivative), Dstrong, Dhat, VdmInv [n*n]. */
 int esdg_basis(int N, int FluxDifferencing, double* xGL, double* wGL, double* xG, double* wG, double* D, double* D0,
                double* Dstrong, double* Dhat, double* VdmInv);
+
+/* basis::FiniteDifferenceOperators (src/basis.cpp:190-229): the central,
+ * forward and backward two-point difference matrices [n*n] on the LGL
+ * nodes used by the partial-dry volume term. */
+int esdg_basis_fd(int N, double* DCentralFD, double* DforwardFD, double* DbackwardFD);
 
 /* Mesh::GenerateMesh (src/Mesh.cpp:316-696) for a Cartesian grid.
  * periodic_rows / periodic_cols are the reference's PeriodicBD_X /

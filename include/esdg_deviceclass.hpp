@@ -79,8 +79,8 @@ class deviceclass {
               h_, "buildDeviceKernels");
     }
 
-    void copyPartialDryData(const double*, const double*, const double*) {
-        throw std::runtime_error("esdg: PartialDryTreatment is outside the rebuilt path");
+    void copyPartialDryData(const double* DCentralFD, const double* DforwardFD, const double* DbackwardFD) {
+        check(esdg_copy_partial_dry_data(h_, DCentralFD, DforwardFD, DbackwardFD), h_, "copyPartialDryData");
     }
 
     void copyTimeSeriesIDs(const int, const int, const int, const int, const int, const int, const int) {}

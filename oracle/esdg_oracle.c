@@ -742,6 +742,101 @@ static void pos_pres(const oconst* c, int K, const double* EleSizes, const doubl
     }
 }
 
+/* --- okl/PartialDryTreatment/FindDryElements.okl:16-63 -------------------- */
+static void find_dry(const oconst* c, int K, const double* Q, int* dry) {
+    const int ngl = c->ngl, n2 = ngl * ngl;
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < K; ++e) {
+        double mh = 1.0;
+        for (int k = 0; k < ngl; ++k)
+            for (int l = 0; l < ngl; ++l) mh = fmin(Q[(long)e * n2 * NEQ + k * ngl + l], mh);
+        dry[e] = mh < c->PosPresTOL ? 1 : 0;
+    }
+}
+
+/* --- okl/PartialDryTreatment/VolumeKernelFD.okl:33-343: momentum volume
+ * terms of partly dry elements, overwriting Qt[hu], Qt[hv] there (called
+ * right after the volume kernel, src/deviceclass.cpp:987-991).  Row i is
+ * eta, column j is xi; a difference uses a neighbour only where it is wet. */
+static void volume_partial_dry(const oconst* c, int K, const double* Jac, const double* Yxi, const double* Yeta,
+                               const double* Xxi, const double* Xeta, const double* Q, const int* dry,
+                               const double* Dc, const double* Dup, const double* Ddn, const double* B, double* Qt) {
+    const int n = c->ngl, n2 = n * n;
+    const double tol = c->PosPresTOL, g = c->g_const;
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < K; ++e) {
+        if (dry[e] != 1) continue;
+        const double* H = Q + (long)e * n2 * NEQ; /* h of the element, [i][j] */
+        const double* b = B + (long)e * n2;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const int id = i * n + j;
+                const double h = H[id], bb = b[id];
+                const double xm = j > 0 ? H[id - 1] : 0.0, xp = j < n - 1 ? H[id + 1] : 0.0;
+                const double ym = i > 0 ? H[id - n] : 0.0, yp = i < n - 1 ? H[id + n] : 0.0;
+                /* F2_2 = G3_2 = g h; the derivatives of F and G coincide */
+                double dFxi = 0.0, dFeta = 0.0, dBxi = 0.0, dBeta = 0.0;
+                if (h > tol) {
+                    if (j == 0 && xp > tol) {
+                        dFxi = Dup[j * n + 0] * (g * h) + Dup[j * n + 1] * (g * H[id + 1]);
+                        dBxi = Dup[j * n + 0] * bb + Dup[j * n + 1] * b[id + 1];
+                    }
+                    if (j == n - 1 && xm > tol) {
+                        dFxi = Ddn[j * n + n - 2] * (g * H[id - 1]) + Ddn[j * n + n - 1] * (g * h);
+                        dBxi = Ddn[j * n + n - 2] * b[id - 1] + Ddn[j * n + n - 1] * bb;
+                    }
+                    if (j > 0 && j < n - 1) {
+                        if (xp > tol && xm > tol) {
+                            dFxi = Dc[j * n + j - 1] * (g * H[id - 1]) + Dc[j * n + j + 1] * (g * H[id + 1]);
+                            dBxi = Dc[j * n + j - 1] * b[id - 1] + Dc[j * n + j + 1] * b[id + 1];
+                        } else if (xp > tol) {
+                            dFxi = Dup[j * n + j] * (g * h) + Dup[j * n + j + 1] * (g * H[id + 1]);
+                            dBxi = Dup[j * n + j] * bb + Dup[j * n + j + 1] * b[id + 1];
+                        } else if (xm > tol) {
+                            dFxi = Ddn[j * n + j - 1] * (g * H[id - 1]) + Ddn[j * n + j] * (g * h);
+                            dBxi = Ddn[j * n + j - 1] * b[id - 1] + Ddn[j * n + j] * bb;
+                        }
+                    }
+                    if (i == 0 && yp > tol) {
+                        dFeta = Dup[i * n + 0] * (g * h) + Dup[i * n + 1] * (g * H[id + n]);
+                        dBeta = Dup[i * n + 0] * bb + Dup[i * n + 1] * b[id + n];
+                    }
+                    if (i == n - 1 && ym > tol) {
+                        dFeta = Ddn[i * n + n - 2] * (g * H[id - n]) + Ddn[i * n + n - 1] * (g * h);
+                        dBeta = Ddn[i * n + n - 2] * b[id - n] + Ddn[i * n + n - 1] * bb;
+                    }
+                    if (i > 0 && i < n - 1) {
+                        if (yp > tol && ym > tol) {
+                            dFeta = Dc[i * n + i - 1] * (g * H[id - n]) + Dc[i * n + i + 1] * (g * H[id + n]);
+                            dBeta = Dc[i * n + i - 1] * b[id - n] + Dc[i * n + i + 1] * b[id + n];
+                        } else if (yp > tol) {
+                            dFeta = Dup[i * n + i] * (g * h) + Dup[i * n + i + 1] * (g * H[id + n]);
+                            dBeta = Dup[i * n + i] * bb + Dup[i * n + i + 1] * b[id + n];
+                        } else if (ym > tol) {
+                            dFeta = Ddn[i * n + i - 1] * (g * H[id - n]) + Ddn[i * n + i] * (g * h);
+                            dBeta = Ddn[i * n + i - 1] * b[id - n] + Ddn[i * n + i] * bb;
+                        }
+                    }
+                }
+                /* g/2 h^2 at the element's edges */
+                const double pBD = c->half_g * h * h;
+                double bxi = 0.0, beta = 0.0;
+                if (j == 0) bxi += c->geomFace * pBD;
+                if (j == n - 1) bxi += -c->geomFace * pBD;
+                if (i == 0) beta += c->geomFace * pBD;
+                if (i == n - 1) beta += -c->geomFace * pBD;
+                const long x = (long)e * n2 + id;
+                const double ye = Yeta[x], yx = Yxi[x], xe = Xeta[x], xx = Xxi[x], J = Jac[x];
+                const double f2 = h * (ye * dFxi - yx * dFeta) + (ye * bxi - yx * beta);
+                const double f3 = h * (-xe * dFxi + xx * dFeta) + (-xe * bxi + xx * beta);
+                const double bx = ye * dBxi - yx * dBeta, by = -xe * dBxi + xx * dBeta;
+                const long q = (long)e * n2 * NEQ + id;
+                Qt[q + n2] = -J * f2 - g * J * h * bx;
+                Qt[q + 2 * n2] = -J * f3 - g * J * h * by;
+            }
+    }
+}
+
 /* ========================================================================= */
 /* Public entry points                                                        */
 /* ========================================================================= */
@@ -751,6 +846,9 @@ typedef struct {
     const double *Jinv, *Yxi, *Yeta, *Xxi, *Xeta, *Bx, *By, *B, *nx, *ny, *scal;
     const double *D, *Dstrong, *Dhat, *VdmInv, *GLw, *EleSizes;
     const int *EdgeData, *EdgeReversed, *ElemToEdge, *MasterSlave, *Orientation;
+    /* partial-dry treatment (PD = 1): difference matrices (src/basis.cpp:190-229) */
+    const double *DcFD, *DfFD, *DbFD;
+    int PD;
 } oracle_geom;
 
 /* One right-hand-side evaluation Qt = L(q) (no AV), as the stage body of
@@ -771,6 +869,13 @@ void oracle_rhs(int N, int K, int F, double g, double PosPresTOL, int ES, int Nu
     oracle_collect_bottom(F, ngl, G->EdgeData, G->B, bL, bR);
     oracle_collect_edge_walls(F, ngl, G->EdgeData, q, G->nx, G->ny, qL, qR);
     volume_fluxdiff(&c, K, G->Jinv, G->Yxi, G->Yeta, G->Xxi, G->Xeta, q, G->D, G->Bx, G->By, Qt);
+    if (G->PD) {
+        int* dry = (int*)calloc(K, sizeof(int));
+        find_dry(&c, K, q, dry);
+        volume_partial_dry(&c, K, G->Jinv, G->Yxi, G->Yeta, G->Xxi, G->Xeta, q, dry, G->DcFD, G->DfFD, G->DbFD,
+                           G->B, Qt);
+        free(dry);
+    }
     num_fluxes(&c, NumFlux, F, G->EdgeReversed, G->nx, G->ny, G->scal, qL, qR, bL, bR, SP);
     surface_lift(ngl, K, G->Jinv, G->MasterSlave, G->Orientation, G->ElemToEdge, SP, Qt);
     free(qL); free(qR); free(bL); free(bR);
@@ -809,6 +914,7 @@ int oracle_timeloop(int N, int K, int F, const oracle_geom* G, double* q, double
     double* bL = (double*)calloc(nf, sizeof(double));
     double* bR = (double*)calloc(nf, sizeof(double));
     double* SP = (double*)calloc(nf * NEQ, sizeof(double));
+    int* dry = G->PD ? (int*)calloc(K, sizeof(int)) : NULL;
     double *VP = NULL, *GX = NULL, *GY = NULL, *SGX = NULL, *SGY = NULL, *VPL = NULL, *VPR = NULL;
     double *GXL = NULL, *GXR = NULL, *GYL = NULL, *GYR = NULL, *SPV = NULL;
     if (AV) {
@@ -846,6 +952,11 @@ int oracle_timeloop(int N, int K, int F, const oracle_geom* G, double* q, double
         for (int s = 0; s < rkStages; ++s) {
             oracle_collect_edge_walls(F, ngl, G->EdgeData, q, G->nx, G->ny, qL, qR);
             volume_fluxdiff(&c, K, G->Jinv, G->Yxi, G->Yeta, G->Xxi, G->Xeta, q, G->D, G->Bx, G->By, Qt);
+            if (G->PD) {
+                find_dry(&c, K, q, dry);
+                volume_partial_dry(&c, K, G->Jinv, G->Yxi, G->Yeta, G->Xxi, G->Xeta, q, dry, G->DcFD, G->DfFD,
+                                   G->DbFD, G->B, Qt);
+            }
             num_fluxes(&c, NumFlux, F, G->EdgeReversed, G->nx, G->ny, G->scal, qL, qR, bL, bR, SP);
             surface_lift(ngl, K, G->Jinv, G->MasterSlave, G->Orientation, G->ElemToEdge, SP, Qt);
             if (AV) {
@@ -881,7 +992,7 @@ int oracle_timeloop(int N, int K, int F, const oracle_geom* G, double* q, double
     if (steps_out) *steps_out = steps;
     free(Qt); free(gRK); free(Qtmp); free(qL); free(qR); free(bL); free(bR); free(SP);
     free(VP); free(GX); free(GY); free(SGX); free(SGY); free(VPL); free(VPR);
-    free(GXL); free(GXR); free(GYL); free(GYR); free(SPV);
+    free(GXL); free(GXR); free(GYL); free(GYR); free(SPV); free(dry);
     return 0;
 }
 

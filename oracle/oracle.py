@@ -23,7 +23,8 @@ _PI = ctypes.POINTER(ctypes.c_int)
 class _Geom(ctypes.Structure):
     _fields_ = [(n, _PD) for n in ("Jinv", "Yxi", "Yeta", "Xxi", "Xeta", "Bx", "By", "B", "nx", "ny", "scal", "D",
                                    "Dstrong", "Dhat", "VdmInv", "GLw", "EleSizes")] + \
-               [(n, _PI) for n in ("EdgeData", "EdgeReversed", "ElemToEdge", "MasterSlave", "Orientation")]
+               [(n, _PI) for n in ("EdgeData", "EdgeReversed", "ElemToEdge", "MasterSlave", "Orientation")] + \
+               [(n, _PD) for n in ("DcFD", "DfFD", "DbFD")] + [("PD", ctypes.c_int)]
 
 
 _LIB = None
@@ -73,7 +74,11 @@ class OracleProblem:
             assert v.dtype == np.float64 and v.flags.c_contiguous, k
         for k, v in self._ints.items():
             assert v.dtype == np.int32 and v.flags.c_contiguous, k
-        self.g = _Geom(**{k: _p(v) for k, v in self._arrs.items()}, **{k: _p(v, _PI) for k, v in self._ints.items()})
+        pd = int(getattr(prob.params, "PartialDryTreatment", 0))
+        fd = getattr(prob.basis, "fd_mats", None) or prob.basis.fd()
+        self._fd = [np.ascontiguousarray(a, dtype=np.float64) for a in fd]
+        self.g = _Geom(**{k: _p(v) for k, v in self._arrs.items()}, **{k: _p(v, _PI) for k, v in self._ints.items()},
+                       DcFD=_p(self._fd[0]), DfFD=_p(self._fd[1]), DbFD=_p(self._fd[2]), PD=pd)
 
     def rhs(self, q):
         p = self.prob.params

@@ -49,8 +49,9 @@ def build():
     return EXE
 
 
-def seq_names(pp: int):
-    return SEQ_BEFORE_GLW + (["GLw"] if pp else []) + SEQ_AFTER_GLW
+def seq_names(pp: int, pd: int = 0):
+    # copyPartialDryData (main.cpp:938-941) follows copyDeviceVariables
+    return SEQ_BEFORE_GLW + (["GLw"] if pp else []) + SEQ_AFTER_GLW + (["DcFD", "DfFD", "DbFD"] if pd else [])
 
 
 def write_input(path, params, mesh_file="none", cartesian=1):
@@ -65,6 +66,7 @@ def write_input(path, params, mesh_file="none", cartesian=1):
             "NavgPad": params.NavgPad, "KernelVersionFD": 99, "KernelVersionSTD": 99, "DiscBottom": 0,
             "ReadInBottom": 0, "PartialDryTreatment": 0, "FrictionTerms": 0, "ConvertToKM": 0, "ArrivalTimings": 0,
             "createTimeSeries": 0, "maximumElevation": 0}
+    vals["PartialDryTreatment"] = int(getattr(params, "PartialDryTreatment", 0))
     with open(path, "w") as f:
         for k in INPUT_KEYS:
             f.write(f"{k}={vals[k]}\n")
@@ -97,7 +99,7 @@ def run(tag, params, cartesian=None, mesh_file=None, inject=None, mode="Serial",
         write_cartesian(os.path.join(rd, "Cartesian.dat"), *cartesian)
     else:
         write_input(os.path.join(rd, "input.dat"), params, mesh_file, 0)
-    names = seq_names(params.PositivityPreserving)
+    names = seq_names(params.PositivityPreserving, int(getattr(params, "PartialDryTreatment", 0)))
     for k, v in (inject or {}).items():
         np.ascontiguousarray(v, dtype=np.float64).tofile(os.path.join(rd, "inject", f"from_{names.index(k):03d}.bin"))
     env = dict(os.environ)

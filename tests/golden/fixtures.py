@@ -35,6 +35,8 @@ def load(name):
     basis = host.Basis.build(N, p.FluxDifferencing)
     # the matrices the reference used (identical to basis' -- checked by tests)
     basis.D, basis.Dstrong, basis.Dhat, basis.VdmInv = z["D"], z["Dstrong"], z["Dhat"], z["VdmInv"]
+    if "DcFD" in z.files:  # copyPartialDryData's matrices (partial-dry runs)
+        basis.fd_mats = (z["DcFD"], z["DfFD"], z["DbFD"])
     EleSizes = z["EleSizes"]
     minEle = float(np.sqrt(EleSizes.min()))
     prob = host.Problem(p, basis, mesh, z["b"], z["Bx"], z["By"], z["q"], EleSizes, minEle, z["rkA"], z["rkB"],

@@ -149,6 +149,27 @@ def case_ssp_walls(name="walls_ssp3_N2"):
     save(name, params, out, {"mesh": "Cartesian walls 10x8 on [-1,1]x[0,1]", "rk": "SSP-RK3"})
 
 
+
+def case_island_pd(name="island_pd_N3"):
+    """Lake with an island that rises above the surface (h = 0 on the dry
+    top) and a ripple on the water: partial-dry treatment and the
+    positivity limiter on, walls."""
+    N = 3
+    params = host.Params(N=N, CFL=0.3, T=0.01, NumFlux=0, rkOrder=4, rkSSP=0, PositivityPreserving=1,
+                         PosPresTOL=1e-3, PartialDryTreatment=1)
+    m = host.mesh_cartesian(N, 0.0, 1.0, 0.0, 1.0, 12, 12)
+    x, y = m.x, m.y
+    b = 1.4 * np.exp(-((x - 0.47) ** 2 + (y - 0.52) ** 2) / 0.18 ** 2)
+    wet = np.maximum(0.0, 1.0 - b)
+    h = np.where(wet > 0, wet + 0.02 * np.exp(-((x - 0.8) ** 2 + (y - 0.25) ** 2) / 0.1 ** 2), 0.0)
+    basis = host.Basis.build(N)
+    Bx, By = host.bottom_derivatives(m, basis, b)
+    out = run_ref.run(name, params, cartesian=(0.0, 1.0, 0.0, 1.0, 12, 12, 0, 0),
+                      inject={"q": pack_q(h, n2=(N + 1) ** 2), "b": b, "Bx": Bx, "By": By})
+    save(name, params, out, {"mesh": "Cartesian walls 12x12 on [0,1]^2", "state": "island above the surface",
+                             "partial_dry": True})
+
+
 CASES = {
     "periodic_nf0_N3": lambda: case_periodic(0, "periodic_nf0_N3"),
     "periodic_nf3_N3": lambda: case_periodic(3, "periodic_nf3_N3"),
@@ -157,6 +178,7 @@ CASES = {
     "circle_dam_av_N3": lambda: case_circle("circle_dam_av_N3", N=3, AV=1, T=0.005, state="dam"),
     "periodic_pp_N3": lambda: case_positivity(),
     "walls_ssp3_N2": lambda: case_ssp_walls(),
+    "island_pd_N3": lambda: case_island_pd(),
 }
 
 

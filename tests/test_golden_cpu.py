@@ -43,6 +43,25 @@ def test_basis_matches_reference(N):
         np.testing.assert_array_equal(mine, z[k], err_msg=k)
 
 
+def test_partial_dry_matrices_match_reference():
+    """esdg_basis_fd against the matrices the reference handed to
+    copyPartialDryData (basis::FiniteDifferenceOperators)."""
+    _, _, z = fixtures.load("island_pd_N3")
+    Dc, Df, Db = host.Basis.build(3).fd()
+    np.testing.assert_array_equal(Dc, z["DcFD"])
+    np.testing.assert_array_equal(Df, z["DfFD"])
+    np.testing.assert_array_equal(Db, z["DbFD"])
+
+
+def test_partial_dry_changes_the_run():
+    """The island case exercises the treatment: without it the oracle ends
+    elsewhere than the reference."""
+    prob, q_ref, _ = fixtures.load("island_pd_N3")
+    prob.params.PartialDryTreatment = 0
+    out = OracleProblem(prob).run(T=prob.params.T, max_steps=0)
+    assert np.abs(out["q"] - q_ref).max() > 1e-3
+
+
 def _compare_setup(mesh, basis, z, skip=()):
     es, _ = host.element_sizes(mesh, basis)
     pairs = [("nx", mesh.nx), ("ny", mesh.ny), ("scal", mesh.scal), ("x_xi", mesh.x_xi), ("x_eta", mesh.x_eta),

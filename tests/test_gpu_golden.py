@@ -2,8 +2,9 @@
 
 Each golden fixture is a run of the reference itself (tests/golden/); the
 engine starts from the identical copyDeviceVariables arrays and must end
-within relative L2 1e-12 per conserved variable of the reference's state
-(the engine contracts a*b+c into FMA, the reference does not).
+within relative L2 1e-12 per conserved variable of the reference's state;
+on the plain path (no shock sensor) the state must be the reference's bit
+for bit.
 """
 import numpy as np
 import pytest

@@ -1,7 +1,8 @@
 """CUDA engine vs CPU oracle on the same seeded inputs (GPU).
 
-Tolerances (FP64 throughout; the engine contracts a*b+c into FMA, the oracle
-does not, so results differ at round-off and grow slowly with the steps):
+Tolerances (FP64 throughout; both sides round every operation without FMA
+contraction, so most cases agree bit for bit, but the bounds below are the
+contract):
   * one right-hand side:        max|dQt| <= 1e-13 * S per variable, S the
                                 largest term that enters it (max|Qt|, g*h*|grad b|,
                                 and 1), since the flux and source terms cancel
