@@ -218,6 +218,8 @@ def main():
     ap.add_argument("--rates", default="10,100,1000", help="serving workload: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=48, help="serving workload: requests per rate")
     ap.add_argument("--hbm-gb", type=float, default=40.0, help="serving workload: HBM given to the arenas")
+    ap.add_argument("--max-live-nodes", type=float, default=2e6,
+                    help="serving workload, shortest-job-first run: nodes in flight at most")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--alone-members", type=int, default=15,
                     help="ensemble workload: members solved one at a time for the plain-path rate")
@@ -529,11 +531,17 @@ def serving_bench(args):
     out = []
     with Clocks(local) as ck:
         for rate in rates:
+            srv.max_live_nodes = None
             b = serving.serve(serving.fresh(streams[rate]), srv, realtime=True)
+            srv.max_live_nodes = int(args.max_live_nodes)
+            j = serving.serve(serving.fresh(streams[rate]), srv, realtime=True, policy="sjf")
+            srv.max_live_nodes = None
             a = serving.serve_one_at_a_time(serving.fresh(streams[rate]), indicator=0, device_id=local)
-            out.append({"rate_per_s": rate, "batched": b, "plain_one_at_a_time": a,
+            out.append({"rate_per_s": rate, "batched": b, "batched_sjf_capped": j, "plain_one_at_a_time": a,
                         "throughput_ratio": b["throughput_dof_stages_per_s"] / a["throughput_dof_stages_per_s"],
-                        "p99_ratio": a["p99_s"] / b["p99_s"]})
+                        "p99_ratio": a["p99_s"] / b["p99_s"],
+                        "sjf_p50_ratio": a["p50_s"] / j["p50_s"], "sjf_p99_ratio": a["p99_s"] / j["p99_s"],
+                        "sjf_throughput_ratio": j["throughput_dof_stages_per_s"] / a["throughput_dof_stages_per_s"]})
         srv.close()
         # the same server architecture with the exact modal active set
         srv1 = serving.Server(hbm_bytes=args.hbm_gb * 1e9, max_instances=256, device_id=local, indicator=1)
@@ -547,7 +555,8 @@ def serving_bench(args):
             "data": "synthetic (seeded tsunami requests, Poisson arrivals)",
             "config": {"workload": f"serving: {args.requests} requests per rate, K in 32^2..256^2, N in {{3,4}}, "
                                    "200-2000 steps, continuous batching with admission by HBM footprint "
-                                   f"({args.hbm_gb} GB of arenas), learned indicator + active set",
+                                   f"({args.hbm_gb} GB of arenas), learned indicator + active set; FIFO, and "
+                                   f"shortest job first with at most {args.max_live_nodes:.0f} nodes in flight",
                        "setup_s": setup_s, "value_is": f"batched throughput at {rates[-1]} requests/s"},
             "rates": out, "batched_modal_active_set_at_top_rate": m1, "clocks": ck.result}
     if rank == 0:

@@ -9,6 +9,14 @@ for the whole arena, each request with its own time step), and retires each
 request the moment its horizon is reached -- freeing its capacity for the
 next one while the others keep running.  No counterpart in the reference.
 
+Admission order: first-in first-out (a request that does not fit blocks the
+later ones of its degree), or shortest job first (waiting requests ordered
+by their work, K (N+1)^2 x 5 x steps DOF-stages, each admitted as soon as it
+fits).  A cap on the nodes in flight (`max_live_nodes`) keeps the GPU
+busy without spreading it over more requests than it needs: once one
+request fills the GPU, every further concurrent request only slows all of
+them down.
+
 The one-at-a-time baseline serves the same stream first-in first-out with
 one single-mesh solver per request (the plain path: modal sensor and viscous
 terms on every element).
@@ -57,6 +65,10 @@ class Request:
     def dof_stages(self) -> float:
         return float(self.nel * self.nel * (self.N + 1) ** 2 * 5 * self.steps)
 
+    @property
+    def nodes(self) -> int:
+        return self.nel * self.nel * (self.N + 1) ** 2
+
 
 def make_requests(n: int, rate: float, seed: int = 0, sizes=SIZES, degrees=DEGREES, horizons=HORIZONS,
                   build: bool = True) -> list[Request]:
@@ -98,10 +110,13 @@ class Server:
 
     def __init__(self, hbm_bytes: float | None = None, degrees=DEGREES, max_instances: int = 256,
                  indicator: int = 2, device_id: int = -1, chunk: int = 4, params: Problem | None = None,
-                 elements: int | None = None):
+                 elements: int | None = None, max_live_nodes: int | None = None):
         """Arena capacity per degree from an HBM budget (split evenly across
-        the degrees), or `elements` per arena directly."""
+        the degrees), or `elements` per arena directly.  max_live_nodes:
+        admit a request only while the nodes of the live requests stay
+        within this (a request is always admitted into an idle server)."""
         self.chunk = chunk
+        self.max_live_nodes = max_live_nodes
         self.arenas: dict[int, Ensemble] = {}
         self.live: dict[int, dict[int, Request]] = {}
         p = (params or problems.tsunami_member(0, sizes=(8,))).params
@@ -123,7 +138,12 @@ class Server:
     def capacity(self):
         return {N: en.free_capacity() for N, en in self.arenas.items()}
 
+    def live_nodes(self) -> int:
+        return sum(r.nodes for live in self.live.values() for r in live.values())
+
     def try_admit(self, r: Request, now: float) -> bool:
+        if self.max_live_nodes is not None and self.busy() and self.live_nodes() + r.nodes > self.max_live_nodes:
+            return False
         en = self.arenas[r.N]
         K, F = r.prob.K, r.prob.F
         ke, kf, slots = en.free_capacity()
@@ -164,9 +184,12 @@ class Server:
         self.arenas.clear()
 
 
-def serve(requests: list[Request], server: Server, realtime: bool = True) -> dict:
-    """Serves the stream: arrivals in (wall-clock) time, FIFO admission by
-    free capacity, continuous batching.  Returns latency statistics."""
+def serve(requests: list[Request], server: Server, realtime: bool = True, policy: str = "fifo") -> dict:
+    """Serves the stream: arrivals in (wall-clock) time, admission by free
+    capacity in FIFO or shortest-job-first order, continuous batching.
+    Returns latency statistics."""
+    if policy not in ("fifo", "sjf"):
+        raise ValueError("policy must be 'fifo' or 'sjf'")
     t0 = time.perf_counter()
 
     def now():
@@ -181,14 +204,19 @@ def serve(requests: list[Request], server: Server, realtime: bool = True) -> dic
         while k < len(pending) and pending[k].arrival <= t:
             waiting.append(pending[k])
             k += 1
-        # FIFO admission (a request that does not fit blocks the ones behind
-        # it of the same degree, so large requests are not starved)
-        blocked = set()
         rest = []
-        for r in waiting:
-            if r.N in blocked or not server.try_admit(r, now()):
-                blocked.add(r.N)
-                rest.append(r)
+        if policy == "fifo":
+            # a request that does not fit blocks the ones behind it of the
+            # same degree, so large requests are not starved
+            blocked = set()
+            for r in waiting:
+                if r.N in blocked or not server.try_admit(r, now()):
+                    blocked.add(r.N)
+                    rest.append(r)
+        else:
+            for r in sorted(waiting, key=lambda r: (r.dof_stages(), r.arrival)):
+                if not server.try_admit(r, now()):
+                    rest.append(r)
         waiting = rest
         if server.busy():
             finished.extend(server.step(now))

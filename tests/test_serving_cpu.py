@@ -86,3 +86,41 @@ def test_fifo_admission_and_continuous_batching():
     # continues across retirements
     assert order.index(("admit", 4)) < order.index(("done", 0))
     assert all(r.latency >= 0 for r in reqs)
+
+
+def test_shortest_job_first_order():
+    # all arrive at t=0; capacity for one request at a time per degree
+    reqs = _reqs([(3, 100, 4), (3, 100, 1), (3, 100, 2)])
+    srv = FakeServer({3: 100})
+    serving.serve(reqs, srv, realtime=False, policy="sjf")
+    admits = [rid for kind, rid in srv.log if kind == "admit"]
+    assert admits == [1, 2, 0]      # by work (steps at equal size)
+    fifo = FakeServer({3: 100})
+    serving.serve(serving.fresh(reqs), fifo, realtime=False, policy="fifo")
+    assert [rid for kind, rid in fifo.log if kind == "admit"] == [0, 1, 2]
+
+
+class _FakeArena:
+    def __init__(self, K):
+        self.K, self.n = K, 0
+
+    def free_capacity(self):
+        return self.K, 2 * self.K, 8
+
+    def add(self, prob, T=None, max_steps=None):
+        self.K -= prob.K
+        self.n += 1
+        return self.n
+
+
+def test_live_node_cap():
+    srv = serving.Server.__new__(serving.Server)
+    srv.arenas = {3: _FakeArena(10 ** 6)}
+    srv.live = {3: {}}
+    srv.max_live_nodes = 2 * 64 * 64 * 16
+    a, b, c = _reqs([(3, 64 * 64, 5), (3, 64 * 64, 5), (3, 64 * 64, 5)])
+    assert srv.try_admit(a, 0.0) and srv.try_admit(b, 0.0)
+    assert not srv.try_admit(c, 0.0)        # would exceed the nodes in flight
+    srv.live[3].clear()
+    big = _reqs([(3, 256 * 256, 5)])[0]
+    assert srv.try_admit(big, 0.0)          # an idle server admits any request that fits
