@@ -218,7 +218,7 @@ def main():
     ap.add_argument("--rates", default="10,100,1000", help="serving workload: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=48, help="serving workload: requests per rate")
     ap.add_argument("--hbm-gb", type=float, default=40.0, help="serving workload: HBM given to the arenas")
-    ap.add_argument("--max-live-nodes", type=float, default=2e6,
+    ap.add_argument("--max-live-nodes", type=float, default=4e6,
                     help="serving workload, shortest-job-first run: nodes in flight at most")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--alone-members", type=int, default=15,

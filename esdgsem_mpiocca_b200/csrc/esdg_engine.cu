@@ -386,22 +386,51 @@ class Engine {
     }
 
     // ---- kernel launchers (dispatch on ngl) ----
+    // Blocks of a face-node (or element-warp) kernel over n threads: one pass
+    // for a single mesh; for an arena a resident grid that strides over the
+    // live extent (the capacity can be far above the live part).
+    int face_blocks(long n) {
+        const int all = (int)((n + 255) / 256);
+        if (!elem_inst) return all;
+        if (n_sms <= 0 && cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+            n_sms = 148;
+        return std::max(1, std::min(all, n_sms * 8));
+    }
+    int n_sms = 0;
+
+    template <int NGL, bool STRIDE>
+    void launch_face_k(const FaceArgs& a, bool av_grad, int blocks) {
+        if (av_grad) {
+            if (NumFlux == 0) k_face_flux<NGL, 0, true, STRIDE><<<blocks, 256, 0, stream>>>(a);
+            else if (NumFlux == 2) k_face_flux<NGL, 2, true, STRIDE><<<blocks, 256, 0, stream>>>(a);
+            else k_face_flux<NGL, 3, true, STRIDE><<<blocks, 256, 0, stream>>>(a);
+        } else {
+            if (NumFlux == 0) k_face_flux<NGL, 0, false, STRIDE><<<blocks, 256, 0, stream>>>(a);
+            else if (NumFlux == 2) k_face_flux<NGL, 2, false, STRIDE><<<blocks, 256, 0, stream>>>(a);
+            else k_face_flux<NGL, 3, false, STRIDE><<<blocks, 256, 0, stream>>>(a);
+        }
+    }
+
+    // viscous face flux, one-shot for a single mesh, strided for an arena
+    template <int NGL>
+    void launch_face_visc(long n, const int* actp, const int* ext) {
+        if (elem_inst)
+            k_face_visc<NGL, true><<<face_blocks(n), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
+                                                                      elem_inst, st, geomFace, actp, ext);
+        else
+            k_face_visc<NGL, false><<<face_blocks(n), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
+                                                                       elem_inst, st, geomFace, actp, ext);
+    }
+
     template <int NGL>
     int launch_face(bool av_grad) {
         FaceArgs a{F, ftab, q, nx, ny, scal, bL, bR, SP, SGX, SGY, elem_inst, st, phys()};
         a.act = (AV && indicator) ? act : nullptr;
         a.extent = extent;
         const long n = (long)F * NGL;
-        const int blocks = (int)((n + 255) / 256);
-        if (av_grad) {
-            if (NumFlux == 0) k_face_flux<NGL, 0, true><<<blocks, 256, 0, stream>>>(a);
-            else if (NumFlux == 2) k_face_flux<NGL, 2, true><<<blocks, 256, 0, stream>>>(a);
-            else k_face_flux<NGL, 3, true><<<blocks, 256, 0, stream>>>(a);
-        } else {
-            if (NumFlux == 0) k_face_flux<NGL, 0, false><<<blocks, 256, 0, stream>>>(a);
-            else if (NumFlux == 2) k_face_flux<NGL, 2, false><<<blocks, 256, 0, stream>>>(a);
-            else k_face_flux<NGL, 3, false><<<blocks, 256, 0, stream>>>(a);
-        }
+        const int blocks = face_blocks(n);
+        if (elem_inst) launch_face_k<NGL, true>(a, av_grad, blocks);
+        else launch_face_k<NGL, false>(a, av_grad, blocks);
         ++launches;
         return 0;
     }
@@ -623,8 +652,7 @@ class Engine {
             launch_elem_plain<NGL>(ea);
             k_grad_list<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
             const long n = (long)F * NGL;
-            k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
-                                                                         elem_inst, st, geomFace, act, extent);
+            launch_face_visc<NGL>(n, act, extent);
             k_element_av2<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
             launches += 3;
         } else if (!AV) {
@@ -638,8 +666,7 @@ class Engine {
             launch_face<NGL>(true);
             k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, A, Bc, C, 0));
             const long n = (long)F * NGL;
-            k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
-                                                                         elem_inst, st, geomFace);
+            launch_face_visc<NGL>(n, nullptr, nullptr);
             k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, A, Bc, C, lam_in_elem));
             launches += 3;
         }
@@ -683,7 +710,7 @@ class Engine {
                 if constexpr ((32 % (NGL * NGL)) == 0)
                     k_ind_features<NGL><<<std::min(ntiles, ind_grid[0]), S::THREADS, 0, stream>>>(ia, ntiles);
                 else
-                    k_ind_features_warp<NGL><<<(K + 7) / 8, 256, 0, stream>>>(ia);
+                    k_ind_features_warp<NGL><<<face_blocks((long)K * 32), 256, 0, stream>>>(ia);
                 k_mlp_forward<KP><<<mlp_grid, 128, MlpSmem<KP>::fwd_bytes(4), stream>>>(K, indX, mlpP, mlpPb, ind_y,
                                                                                  ia.L, extent);
                 k_indicator<NGL, true><<<std::min(ntiles, ind_grid[1]), S::THREADS, 0, stream>>>(ia, ntiles);
@@ -1017,8 +1044,7 @@ class Engine {
                 if (s > 0) launch_indicator<NGL>(0);
                 k_element_av1<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(2, gA[s], gB[s], gC[s], 0));
                 const long n = (long)F * NGL;
-                k_face_visc<NGL><<<(int)((n + 255) / 256), 256, 0, stream>>>(F, ftab, nx, ny, scal, GX, GY, VP, SPV,
-                                                                             elem_inst, st, geomFace);
+                launch_face_visc<NGL>(n, nullptr, nullptr);
                 k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem));
                 launches += 3;
             }

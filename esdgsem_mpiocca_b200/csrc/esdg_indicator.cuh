@@ -186,11 +186,9 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS) k_ind_features(IndArgs
 // (n^2 does not divide 32): one warp per element (nodes lane, lane + 32,
 // ...), the three fields' sums interleaved, no block-wide barrier.
 template <int NGL>
-__global__ void __launch_bounds__(256) k_ind_features_warp(IndArgs a) {
+__device__ __forceinline__ void ind_features_warp_elem(const IndArgs& a, int e) {
     constexpr int N2 = NGL * NGL, R = (N2 + 31) / 32, KP = mlp_kp(NGL);
     const int lane = threadIdx.x & 31;
-    const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (e >= a.K || (a.extent && e >= a.extent[0])) return;  // warp-uniform
     if (a.st[inst_of(a.elem_inst, e)].done) return;
     const double* qe = a.q + (long)e * 3 * N2;
     double v[3][R];
@@ -262,6 +260,15 @@ __global__ void __launch_bounds__(256) k_ind_features_warp(IndArgs a) {
         a.energy[e] = e2;
         a.ok[e] = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
     }
+}
+
+// Warps stride over the elements below the live extent (one pass per warp
+// with the one-shot grid of a single mesh, a resident grid for an arena).
+template <int NGL>
+__global__ void __launch_bounds__(256) k_ind_features_warp(IndArgs a) {
+    const int lim = a.extent ? min(a.K, a.extent[0]) : a.K;
+    for (int e = blockIdx.x * 8 + (threadIdx.x >> 5); e < lim; e += gridDim.x * 8)  // warp-uniform
+        ind_features_warp_elem<NGL>(a, e);
 }
 
 // The learned decision for one element: 1 when the modal sensor must decide.

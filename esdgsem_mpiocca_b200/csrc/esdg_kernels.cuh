@@ -109,12 +109,10 @@ __device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return ele
 // ---------------------------------------------------------------------------
 // Face kernel.
 // ---------------------------------------------------------------------------
+// One face node (gid = face * NGL + node) of the face kernel.
 template <int NGL, int NUMFLUX, bool AV>
-__global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
-    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long)a.F * NGL) return;
+__device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
     const int f = (int)(gid / NGL), i = (int)(gid % NGL);
-    if (a.extent && f >= a.extent[1]) return;
     constexpr int N2 = NGL * NGL;
     const int4 t = a.ftab[f];
     // the face's own data does not depend on the table entry: requested
@@ -169,22 +167,35 @@ __global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
     }
 }
 
+// STRIDE = false: one thread per face node (a single mesh's one-shot
+// grid).  STRIDE = true: a resident grid strides over the face nodes below
+// the live extent (an arena, whose face capacity can be far above its live
+// faces); a separate instantiation, since the loop costs registers.
+template <int NGL, int NUMFLUX, bool AV, bool STRIDE = false>
+__global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
+    long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long all = (long)a.F * NGL;
+    if (!STRIDE) {
+        if (gid >= all || (a.extent && gid >= (long)a.extent[1] * NGL)) return;
+        face_flux_node<NGL, NUMFLUX, AV>(a, gid);
+    } else {
+        const long n = a.extent ? min(all, (long)a.extent[1] * NGL) : all;
+        for (; gid < n; gid += (long)gridDim.x * blockDim.x) face_flux_node<NGL, NUMFLUX, AV>(a, gid);
+    }
+}
+
 // Viscous face flux from the lifted gradients of both elements
 // (okl/BR1_Gradient/CollectEdgeDataGradient.okl:17-194 and
 // okl/ViscoseParts/calcNumFluxesViscose.okl:17-107); zero on walls.
 template <int NGL>
-__global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict__ ftab, const double* __restrict__ nxa,
-                                                   const double* __restrict__ nya, const double* __restrict__ scal,
-                                                   const double* __restrict__ GX, const double* __restrict__ GY,
-                                                   const double* __restrict__ VP, double* __restrict__ SPV,
-                                                   const int* __restrict__ elem_inst, const DevState* __restrict__ st,
-                                                   double geomFace, const int* __restrict__ act = nullptr,
-                                                   const int* __restrict__ extent = nullptr) {
-    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long)F * NGL) return;
+__device__ __forceinline__ void face_visc_node(long gid, const int4* __restrict__ ftab, const double* __restrict__ nxa,
+                                               const double* __restrict__ nya, const double* __restrict__ scal,
+                                               const double* __restrict__ GX, const double* __restrict__ GY,
+                                               const double* __restrict__ VP, double* __restrict__ SPV,
+                                               const int* __restrict__ elem_inst, const DevState* __restrict__ st,
+                                               double geomFace, const int* __restrict__ act) {
     constexpr int N2 = NGL * NGL;
     const int f = (int)(gid / NGL), i = (int)(gid % NGL);
-    if (extent && f >= extent[1]) return;
     const int4 t = ftab[f];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
     if (st[inst_of(elem_inst, eL)].done) return;
@@ -214,6 +225,27 @@ __global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict
     const double s = scal[ex];
     SPV[(long)f * 2 * NGL + i] = -s * geomFace * N0;
     SPV[(long)f * 2 * NGL + NGL + i] = -s * geomFace * N1;
+}
+
+// One-shot or grid-stride over the face nodes (as k_face_flux).
+template <int NGL, bool STRIDE = false>
+__global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict__ ftab, const double* __restrict__ nxa,
+                                                   const double* __restrict__ nya, const double* __restrict__ scal,
+                                                   const double* __restrict__ GX, const double* __restrict__ GY,
+                                                   const double* __restrict__ VP, double* __restrict__ SPV,
+                                                   const int* __restrict__ elem_inst, const DevState* __restrict__ st,
+                                                   double geomFace, const int* __restrict__ act = nullptr,
+                                                   const int* __restrict__ extent = nullptr) {
+    long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long all = (long)F * NGL;
+    if (!STRIDE) {
+        if (gid >= all || (extent && gid >= (long)extent[1] * NGL)) return;
+        face_visc_node<NGL>(gid, ftab, nxa, nya, scal, GX, GY, VP, SPV, elem_inst, st, geomFace, act);
+    } else {
+        const long n = extent ? min(all, (long)extent[1] * NGL) : all;
+        for (; gid < n; gid += (long)gridDim.x * blockDim.x)
+            face_visc_node<NGL>(gid, ftab, nxa, nya, scal, GX, GY, VP, SPV, elem_inst, st, geomFace, act);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -110,12 +110,19 @@ class Server:
 
     def __init__(self, hbm_bytes: float | None = None, degrees=DEGREES, max_instances: int = 256,
                  indicator: int = 2, device_id: int = -1, chunk: int = 4, params: Problem | None = None,
-                 elements: int | None = None, max_live_nodes: int | None = None):
+                 elements: int | None = None, max_live_nodes: int | None = None,
+                 chunk_node_steps: float = 2e7, max_chunk: int = 64):
         """Arena capacity per degree from an HBM budget (split evenly across
         the degrees), or `elements` per arena directly.  max_live_nodes:
         admit a request only while the nodes of the live requests stay
-        within this (a request is always admitted into an idle server)."""
+        within this (a request is always admitted into an idle server).
+        Steps per host poll: at least `chunk`, and with little work in
+        flight up to `max_chunk`, so that a poll covers about
+        `chunk_node_steps` node updates (the poll's host round trip is then
+        small against the GPU time it covers)."""
         self.chunk = chunk
+        self.chunk_node_steps = chunk_node_steps
+        self.max_chunk = max_chunk
         self.max_live_nodes = max_live_nodes
         self.arenas: dict[int, Ensemble] = {}
         self.live: dict[int, dict[int, Request]] = {}
@@ -162,8 +169,10 @@ class Server:
         retires the finished ones (results copied out, capacity freed)."""
         done = []
         running = [N for N in self.arenas if self.live[N]]
+        live = max(self.live_nodes(), 1)
+        chunk = max(self.chunk, min(self.max_chunk, int(self.chunk_node_steps / live)))
         for N in running:  # the arenas run concurrently, each on its own stream
-            self.arenas[N].launch(self.chunk)
+            self.arenas[N].launch(chunk)
         for N in running:
             en = self.arenas[N]
             en.sync()
