@@ -394,7 +394,7 @@ class Engine {
         if (!elem_inst) return all;
         if (n_sms <= 0 && cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
             n_sms = 148;
-        return std::max(1, std::min(all, n_sms * 8));
+        return std::max(1, std::min(all, n_sms * 4));  // the strided kernels' resident blocks
     }
     int n_sms = 0;
 

@@ -172,7 +172,7 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
 // the live extent (an arena, whose face capacity can be far above its live
 // faces); a separate instantiation, since the loop costs registers.
 template <int NGL, int NUMFLUX, bool AV, bool STRIDE = false>
-__global__ void __launch_bounds__(256) k_face_flux(FaceArgs a) {
+__global__ void __launch_bounds__(256, STRIDE ? 4 : 1) k_face_flux(FaceArgs a) {
     long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long all = (long)a.F * NGL;
     if (!STRIDE) {
@@ -229,7 +229,7 @@ __device__ __forceinline__ void face_visc_node(long gid, const int4* __restrict_
 
 // One-shot or grid-stride over the face nodes (as k_face_flux).
 template <int NGL, bool STRIDE = false>
-__global__ void __launch_bounds__(256) k_face_visc(int F, const int4* __restrict__ ftab, const double* __restrict__ nxa,
+__global__ void __launch_bounds__(256, STRIDE ? 4 : 1) k_face_visc(int F, const int4* __restrict__ ftab, const double* __restrict__ nxa,
                                                    const double* __restrict__ nya, const double* __restrict__ scal,
                                                    const double* __restrict__ GX, const double* __restrict__ GY,
                                                    const double* __restrict__ VP, double* __restrict__ SPV,
