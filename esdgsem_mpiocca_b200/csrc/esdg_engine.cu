@@ -154,6 +154,10 @@ class Engine {
     unsigned long long* ind_stats = nullptr;  // [4] decision counts
     std::vector<double> Vinv_h;
     std::vector<double> Dfd_h;  // flux-differencing matrix (host copy, row kernel parameter)
+    // Testcase 1 (manufactured solution): exact boundary states and source
+    // at the stage time t + stage_tfrac dt
+    int conv = 0;
+    double stage_tfrac = 0.0;
     // partial-dry treatment: per-element dry flag, difference matrices
     int* dry = nullptr;
     double *DcFD = nullptr, *DupFD = nullptr, *DdnFD = nullptr;
@@ -349,8 +353,13 @@ class Engine {
             return fail(ESDG_E_UNSUPPORTED, "FluxDifferencing=0 (standard DGSEM volume kernel) is not rebuilt");
         if (NumFlux_ != 0 && NumFlux_ != 2 && NumFlux_ != 3)
             return fail(ESDG_E_UNSUPPORTED, "NumFlux must be 0 (ES), 2 (Rusanov-type ES) or 3 (rotated ES)");
+        conv = 0;
         switch (Testcase_) {
-            case 1: case 8: case 88: case 89: case 6: case 32: case 90: case 91:
+            case 1:  // manufactured solution: Dirichlet boundary states + source (plain path)
+                if (AV_) return fail(ESDG_E_UNSUPPORTED, "Testcase 1 is rebuilt without artificial viscosity");
+                conv = 1;
+                break;
+            case 8: case 88: case 89: case 6: case 32: case 90: case 91:
                 return fail(ESDG_E_UNSUPPORTED, "this Testcase needs a boundary kernel other than SolidWalls");
             default: break;
         }
@@ -427,6 +436,7 @@ class Engine {
         FaceArgs a{F, ftab, q, nx, ny, scal, bL, bR, SP, SGX, SGY, elem_inst, st, phys()};
         a.act = (AV && indicator) ? act : nullptr;
         a.extent = extent;
+        if (conv) { a.conv = 1; a.tfrac = stage_tfrac; a.X = X; a.Y = Y; }
         const long n = (long)F * NGL;
         const int blocks = face_blocks(n);
         if (elem_inst) launch_face_k<NGL, true>(a, av_grad, blocks);
@@ -445,6 +455,7 @@ class Engine {
         if (PartialDry) {
             a.dry = dry; a.Bn = B; a.Dc = DcFD; a.Dup = DupFD; a.Ddn = DdnFD;
         }
+        if (conv) { a.conv = 1; a.tfrac = stage_tfrac; a.X = X; a.Y = Y; }
         return a;
     }
 
@@ -822,6 +833,16 @@ class Engine {
         return 0;
     }
 
+    // Stage time t + fraction * dt (src/deviceclass.cpp:944-952): the LS-RK
+    // B coefficients, {0, 1, 1/2} for SSP-RK3.
+    double stage_time_fraction(int s) const {
+        if (rkSSP) {
+            static const double d[3] = {0.0, 1.0, 0.5};
+            return s < 3 ? d[s] : 0.0;
+        }
+        return gB[s];
+    }
+
     template <int NGL>
     void launch_step() {
         if (AV) launch_indicator<NGL>(1);
@@ -831,8 +852,11 @@ class Engine {
             // o_Qtmp.copyFrom(o_q) (src/deviceclass.cpp:933-936)
             cudaMemcpyAsync(Qtmp, q, (size_t)K * ngl * ngl * 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream);
         }
-        for (int s = 0; s < gStages; ++s)
+        for (int s = 0; s < gStages; ++s) {
+            stage_tfrac = stage_time_fraction(s);
             launch_stage<NGL>(rkSSP ? 1 : 0, gA[s], gB[s], gC[s], s == gStages - 1, s > 0);
+        }
+        stage_tfrac = 0.0;
         k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
         ++launches;
     }
@@ -1034,6 +1058,7 @@ class Engine {
             const bool last = s == gStages - 1;
             const int mode = rkSSP ? 1 : 0;
             const int lam_in_elem = (last && !PP) ? 1 : 0;
+            stage_tfrac = stage_time_fraction(s);
             launch_find_dry<NGL>();
             cudaEventRecord(pev[0], stream);
             launch_face<NGL>(AV != 0);

@@ -54,6 +54,12 @@ struct FaceArgs {
     // live extent (null: all): [0] elements, [1] faces below which every
     // live entity lies (the arena keeps it current between replays)
     const int* __restrict__ extent = nullptr;
+    // Testcase 1 (conv = 1): exact outer states on boundary faces at the
+    // stage time t + tfrac dt, from the nodal coordinates X, Y
+    int conv = 0;
+    double tfrac = 0.0;
+    const double* __restrict__ X = nullptr;
+    const double* __restrict__ Y = nullptr;
 };
 
 struct ElemArgs {
@@ -102,7 +108,24 @@ struct ElemArgs {
     const double* __restrict__ Dc = nullptr;
     const double* __restrict__ Dup = nullptr;
     const double* __restrict__ Ddn = nullptr;
+    // Testcase 1 (conv = 1): the manufactured source at the stage time
+    // t + tfrac dt from the nodal coordinates X, Y (b: B, its derivatives:
+    // Bx, By)
+    int conv = 0;
+    double tfrac = 0.0;
+    const double* __restrict__ X = nullptr;
+    const double* __restrict__ Y = nullptr;
 };
+
+// r += the manufactured source of node xid (Testcase 1).
+__device__ __forceinline__ void add_conv_source(const ElemArgs& a, const DevState& S, long xid, double Bx, double By,
+                                                double& r0, double& r1, double& r2) {
+    double s0, s1, s2;
+    conv_source(a.c.g, a.X[xid], a.Y[xid], S.t + a.tfrac * S.dt, Bx, By, a.B[xid], s0, s1, s2);
+    r0 += s0;
+    r1 += s1;
+    r2 += s2;
+}
 
 __device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return elem_inst ? elem_inst[e] : 0; }
 
@@ -120,7 +143,8 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
     const long ex = (long)f * NGL + i;
     const double nx = a.nx[ex], ny = a.ny[ex], sc = a.scal[ex], bLx = a.bL[ex];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
-    if (a.st[inst_of(a.elem_inst, eL)].done) return;
+    const DevState& S = a.st[inst_of(a.elem_inst, eL)];
+    if (S.done) return;
     const int ir = same ? i : NGL - 1 - i;
     const double* qe = a.q + (long)eL * 3 * N2;
     const int oL = trace_offset(sL, i, NGL);
@@ -141,7 +165,12 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
         // it back at node ir (okl/GatherEdgeData/SolidWalls.okl:150-173).
         const long exr = (long)f * NGL + ir;
         const int o = trace_offset(sL, ir, NGL);
-        wall_ghost(a.nx[exr], a.ny[exr], qe[o], qe[o + N2], qe[o + 2 * N2], hR, huR, hvR);
+        if (a.conv) {  // okl/GatherEdgeData/Dirichlet_ConvTest.okl:112-119, read back the same way
+            const long xo = (long)eL * N2 + o;
+            conv_exact(a.X[xo], a.Y[xo], S.t + a.tfrac * S.dt, a.bL[exr], hR, huR, hvR);
+        } else {
+            wall_ghost(a.nx[exr], a.ny[exr], qe[o], qe[o + N2], qe[o + 2 * N2], hR, huR, hvR);
+        }
         if (grad) { ghR = hL; ghuR = huL; ghvR = hvL; }
     }
     double N0, N1, N2f;
@@ -391,6 +420,7 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
                 r2 += -m * J * f[pass][2] + J * db;
             }
         }
+        if (a.conv) add_conv_source(a, a.st[ins], xid, bx, by, r0, r1, r2);
         if (a.mode == 2 || to_list) {
             a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
             if (to_list && nd == 0) a.alist[atomicAdd(a.acount, 1)] = e;

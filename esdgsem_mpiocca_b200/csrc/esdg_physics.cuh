@@ -196,6 +196,32 @@ __device__ __forceinline__ int trace_offset(int side, int i, int ngl) {
     }
 }
 
+// Testcase 1 (manufactured solution on a Cartesian mesh with Dirichlet
+// boundaries): H = 8 + cos x sin y cos t, u = 1/2, v = 3/2, h = H - b.
+// The exact state (okl/GatherEdgeData/Dirichlet_ConvTest.okl:14-26), used as
+// the outer state of boundary faces at the stage time.
+__device__ __forceinline__ void conv_exact(double x, double y, double t, double b, double& q1, double& q2,
+                                           double& q3) {
+    q1 = (8.0 + cos(x) * sin(y) * cos(t) - b);
+    q2 = 0.5 * (8.0 + cos(x) * sin(y) * cos(t) - b);
+    q3 = 1.5 * (8.0 + cos(x) * sin(y) * cos(t) - b);
+}
+
+// Its source term (okl/ManufacturedSolutions/S_ConvTest.okl), added to the
+// right-hand side after the volume and surface terms, before the update.
+__device__ __forceinline__ void conv_source(double g, double x, double y, double t, double Bx, double By, double B,
+                                            double& s0, double& s1, double& s2) {
+    const double sinY = sin(y), sinX = sin(x), cosY = cos(y), cosX = cos(x);
+    const double H = 8.0 + cosX * sinY * cos(t);
+    const double Ht = -cosX * sinY * sin(t);
+    const double Hx = -sinX * sinY * cos(t);
+    const double Hy = cosX * cosY * cos(t);
+    const double u = 0.5, v = 1.5;
+    s0 = Ht + u * (Hx - Bx) + v * (Hy - By);
+    s1 = u * Ht + u * u * (Hx - Bx) + u * v * (Hy - By) + g * Hx * (H - B);
+    s2 = v * Ht + u * v * (Hx - Bx) + v * v * (Hy - By) + g * Hy * (H - B);
+}
+
 // Order-preserving map of non-negative doubles to unsigned 64-bit keys for
 // atomicMax (NaN maps above +inf, so a NaN anywhere shows up in the max).
 __device__ __forceinline__ unsigned long long dbl_key(double v) {

@@ -310,6 +310,7 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
                     r1 += -mx * J * fx[j][1] + J * db;
                     r2 += -mx * J * fx[j][2] + J * db;
                 }
+                if (a.conv) add_conv_source(a, a.st[ins], (long)e * N2 + j * NGL + ln, sBx[s], sBy[s], r0, r1, r2);
                 const long qid = qe + j * NGL;
                 if (a.mode == 2 || to_list) {
                     a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;

@@ -284,6 +284,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
                     r2 += -m * J * f[pass][2] + J * db;
                 }
             }
+            if (a.conv) add_conv_source(a, a.st[ins], (long)e * N2 + nd, sBx[s], sBy[s], r0, r1, r2);
             const long qid = (long)e * 3 * N2 + nd;
             if (a.mode == 2 || to_list) {
                 a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;

@@ -40,6 +40,27 @@ def periodic_bump(N=3, nel=16, NumFlux=2, ES=1, steps=100, CFL=0.4) -> Problem:
     return make_problem(p, m, b, _state(h, K=m.K, n2=n2), {"name": "periodic_bump", "nel": nel})
 
 
+def conv_test(N=3, nel=8, T=0.1, CFL=0.4, NumFlux=0, L=2.0) -> Problem:
+    """The reference's convergence test (Testcase 1, src/SW2D.cpp:312-319 and
+    :829-833): Cartesian mesh on [0, L]^2 with Dirichlet boundaries carrying
+    the exact solution h = 8 + cos x sin y cos t - b, u = 1/2, v = 3/2 over
+    b = 2 + sin(2 pi y)/2 + cos(2 pi x), with the matching source term."""
+    p = Params(N=N, CFL=CFL, T=T, g_const=9.81, NumFlux=NumFlux, ES=1, rkOrder=4, rkSSP=0, Testcase=1)
+    m = mesh_cartesian(N, 0.0, L, 0.0, L, nel, nel)
+    x, y = m.x, m.y
+    b = 2.0 + 0.5 * np.sin(2.0 * np.pi * y) + np.cos(2.0 * np.pi * x)
+    h = 8.0 + np.cos(x) * np.sin(y) - b
+    n2 = (N + 1) ** 2
+    return make_problem(p, m, b, _state(h, 0.5 * h, 1.5 * h, K=m.K, n2=n2), {"name": "conv_test", "nel": nel})
+
+
+def conv_exact(prob, t):
+    """Exact state of conv_test at time t, [K][3][n2] flattened."""
+    m = prob.mesh
+    h = 8.0 + np.cos(m.x) * np.sin(m.y) * np.cos(t) - prob.b
+    return _state(h, 0.5 * h, 1.5 * h, K=m.K, n2=(prob.params.N + 1) ** 2)
+
+
 def gaussian_bumps(x, y, seed, count=8):
     rng = np.random.default_rng(seed)
     b = np.zeros_like(x)

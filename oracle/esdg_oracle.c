@@ -135,6 +135,64 @@ void oracle_collect_edge_walls(int F, int ngl, const int* EdgeData, const double
         }
 }
 
+/* --- Testcase 1: okl/GatherEdgeData/Dirichlet_ConvTest.okl:14-185, the exact
+ * state H = 8 + cos x sin y cos t (minus b), u = 1/2, v = 3/2 outside the
+ * boundary faces at the stage time t. */
+static void conv_qnodal(double x, double y, double t, double b, double* q) {
+    q[0] = (8.0 + cos(x) * sin(y) * cos(t) - b);
+    q[1] = 0.5 * (8.0 + cos(x) * sin(y) * cos(t) - b);
+    q[2] = 1.5 * (8.0 + cos(x) * sin(y) * cos(t) - b);
+}
+
+static void collect_edge_conv(int F, int ngl, const int* EdgeData, const double* Q, const double* X, const double* Y,
+                              const double* bL, const double* bR, double t, double* qL, double* qR) {
+    const int n2 = ngl * ngl;
+#pragma omp parallel for schedule(static)
+    for (int ifa = 0; ifa < F; ++ifa)
+        for (int i = 0; i < ngl; ++i) {
+            const int iel = EdgeData[8 * ifa], ier = EdgeData[8 * ifa + 1];
+            const int isl = EdgeData[8 * ifa + 2], isr = EdgeData[8 * ifa + 3];
+            const int cpuL = EdgeData[8 * ifa + 5], cpuR = EdgeData[8 * ifa + 6];
+            const long eid = (long)ifa * ngl * NEQ + i, ex = (long)ifa * ngl + i;
+            double L[3] = {0, 0, 0}, R[3] = {0, 0, 0};
+            long xl = 0, xr = 0;
+            if (cpuL == 0) {
+                const long id = trace_index(iel, isl, i, ngl, NEQ);
+                xl = trace_index(iel, isl, i, ngl, 1);
+                L[0] = Q[id]; L[1] = Q[id + n2]; L[2] = Q[id + 2 * n2];
+            }
+            if (cpuR == 0) {
+                const long id = trace_index(ier, isr, i, ngl, NEQ);
+                xr = trace_index(ier, isr, i, ngl, 1);
+                R[0] = Q[id]; R[1] = Q[id + n2]; R[2] = Q[id + 2 * n2];
+            }
+            if (cpuL == -1) conv_qnodal(X[xr], Y[xr], t, bR[ex], L);
+            if (cpuR == -1) conv_qnodal(X[xl], Y[xl], t, bL[ex], R);
+            qL[eid] = L[0]; qL[eid + ngl] = L[1]; qL[eid + 2 * ngl] = L[2];
+            qR[eid] = R[0]; qR[eid + ngl] = R[1]; qR[eid + 2 * ngl] = R[2];
+        }
+}
+
+/* --- Testcase 1: okl/ManufacturedSolutions/S_ConvTest.okl (addS) ----------- */
+static void add_conv_source(const oconst* c, int K, const double* Bx, const double* By, const double* B,
+                            const double* X, const double* Y, double t, double* Qt) {
+    const int ngl = c->ngl, n2 = ngl * ngl;
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < K; ++e)
+        for (int k = 0; k < n2; ++k) {
+            const long x = (long)e * n2 + k, id = (long)e * n2 * NEQ + k;
+            const double sinY = sin(Y[x]), sinX = sin(X[x]), cosY = cos(Y[x]), cosX = cos(X[x]);
+            const double H = 8.0 + cosX * sinY * cos(t);
+            const double Ht = -cosX * sinY * sin(t);
+            const double Hx = -sinX * sinY * cos(t);
+            const double Hy = cosX * cosY * cos(t);
+            const double u = 0.5, v = 1.5;
+            Qt[id] += Ht + u * (Hx - Bx[x]) + v * (Hy - By[x]);
+            Qt[id + n2] += u * Ht + u * u * (Hx - Bx[x]) + u * v * (Hy - By[x]) + c->g_const * Hx * (H - B[x]);
+            Qt[id + 2 * n2] += v * Ht + u * v * (Hx - Bx[x]) + v * v * (Hy - By[x]) + c->g_const * Hy * (H - B[x]);
+        }
+}
+
 /* --- okl/DG/VolumeKernelFluxDiffV99.okl:17-57 two-point fluxes ------------- */
 static inline void Fvol(const oconst* c, double q1L, double q2L, double q3L, double qInvL, double q1R, double q2R,
                         double q3R, double qInvR, double YetaL, double YetaR, double XetaL, double XetaR, double* F1,
@@ -849,6 +907,9 @@ typedef struct {
     /* partial-dry treatment (PD = 1): difference matrices (src/basis.cpp:190-229) */
     const double *DcFD, *DfFD, *DbFD;
     int PD;
+    /* Testcase 1 (manufactured solution): nodal coordinates */
+    const double *X, *Y;
+    int Testcase;
 } oracle_geom;
 
 /* One right-hand-side evaluation Qt = L(q) (no AV), as the stage body of
@@ -867,7 +928,10 @@ void oracle_rhs(int N, int K, int F, double g, double PosPresTOL, int ES, int Nu
     double* bR = (double*)calloc(nf, sizeof(double));
     double* SP = SurfaceParts_out ? SurfaceParts_out : (double*)calloc(nf * NEQ, sizeof(double));
     oracle_collect_bottom(F, ngl, G->EdgeData, G->B, bL, bR);
-    oracle_collect_edge_walls(F, ngl, G->EdgeData, q, G->nx, G->ny, qL, qR);
+    if (G->Testcase == 1)
+        collect_edge_conv(F, ngl, G->EdgeData, q, G->X, G->Y, bL, bR, 0.0, qL, qR);
+    else
+        oracle_collect_edge_walls(F, ngl, G->EdgeData, q, G->nx, G->ny, qL, qR);
     volume_fluxdiff(&c, K, G->Jinv, G->Yxi, G->Yeta, G->Xxi, G->Xeta, q, G->D, G->Bx, G->By, Qt);
     if (G->PD) {
         int* dry = (int*)calloc(K, sizeof(int));
@@ -878,6 +942,7 @@ void oracle_rhs(int N, int K, int F, double g, double PosPresTOL, int ES, int Nu
     }
     num_fluxes(&c, NumFlux, F, G->EdgeReversed, G->nx, G->ny, G->scal, qL, qR, bL, bR, SP);
     surface_lift(ngl, K, G->Jinv, G->MasterSlave, G->Orientation, G->ElemToEdge, SP, Qt);
+    if (G->Testcase == 1) add_conv_source(&c, K, G->Bx, G->By, G->B, G->X, G->Y, 0.0, Qt);
     free(qL); free(qR); free(bL); free(bR);
     if (!SurfaceParts_out) free(SP);
 }
@@ -950,7 +1015,14 @@ int oracle_timeloop(int N, int K, int F, const oracle_geom* G, double* q, double
         if (dt_log) dt_log[steps] = dt;
         if (rkSSP) memcpy(Qtmp, q, nd * sizeof(double));
         for (int s = 0; s < rkStages; ++s) {
-            oracle_collect_edge_walls(F, ngl, G->EdgeData, q, G->nx, G->ny, qL, qR);
+            /* stage time (src/deviceclass.cpp:944-952) */
+            static const double rkD[3] = {0.0, 1.0, 0.5};
+            double ts = t;
+            ts += (rkSSP ? rkD[s < 3 ? s : 0] : rkB[s]) * dt;
+            if (G->Testcase == 1)
+                collect_edge_conv(F, ngl, G->EdgeData, q, G->X, G->Y, bL, bR, ts, qL, qR);
+            else
+                oracle_collect_edge_walls(F, ngl, G->EdgeData, q, G->nx, G->ny, qL, qR);
             volume_fluxdiff(&c, K, G->Jinv, G->Yxi, G->Yeta, G->Xxi, G->Xeta, q, G->D, G->Bx, G->By, Qt);
             if (G->PD) {
                 find_dry(&c, K, q, dry);
@@ -970,6 +1042,7 @@ int oracle_timeloop(int N, int K, int F, const oracle_geom* G, double* q, double
                 num_fluxes_viscous(&c, F, G->EdgeData, G->nx, G->ny, G->scal, VPL, VPR, GXL, GXR, GYL, GYR, SPV);
                 surface_lift_visc(ngl, K, G->Jinv, G->MasterSlave, G->Orientation, G->ElemToEdge, SPV, Qt);
             }
+            if (G->Testcase == 1) add_conv_source(&c, K, G->Bx, G->By, G->B, G->X, G->Y, ts, Qt);
             if (rkSSP) {
                 const double A = rkA[s], Bc = rkB[s], C = rkC[s];
 #pragma omp parallel for schedule(static)

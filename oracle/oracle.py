@@ -24,7 +24,8 @@ class _Geom(ctypes.Structure):
     _fields_ = [(n, _PD) for n in ("Jinv", "Yxi", "Yeta", "Xxi", "Xeta", "Bx", "By", "B", "nx", "ny", "scal", "D",
                                    "Dstrong", "Dhat", "VdmInv", "GLw", "EleSizes")] + \
                [(n, _PI) for n in ("EdgeData", "EdgeReversed", "ElemToEdge", "MasterSlave", "Orientation")] + \
-               [(n, _PD) for n in ("DcFD", "DfFD", "DbFD")] + [("PD", ctypes.c_int)]
+               [(n, _PD) for n in ("DcFD", "DfFD", "DbFD")] + [("PD", ctypes.c_int)] + \
+               [(n, _PD) for n in ("X", "Y")] + [("Testcase", ctypes.c_int)]
 
 
 _LIB = None
@@ -77,8 +78,10 @@ class OracleProblem:
         pd = int(getattr(prob.params, "PartialDryTreatment", 0))
         fd = getattr(prob.basis, "fd_mats", None) or prob.basis.fd()
         self._fd = [np.ascontiguousarray(a, dtype=np.float64) for a in fd]
+        self._xy = [np.ascontiguousarray(a, dtype=np.float64) for a in (m.x, m.y)]
         self.g = _Geom(**{k: _p(v) for k, v in self._arrs.items()}, **{k: _p(v, _PI) for k, v in self._ints.items()},
-                       DcFD=_p(self._fd[0]), DfFD=_p(self._fd[1]), DbFD=_p(self._fd[2]), PD=pd)
+                       DcFD=_p(self._fd[0]), DfFD=_p(self._fd[1]), DbFD=_p(self._fd[2]), PD=pd,
+                       X=_p(self._xy[0]), Y=_p(self._xy[1]), Testcase=int(prob.params.Testcase))
 
     def rhs(self, q):
         p = self.prob.params

@@ -170,6 +170,18 @@ def case_island_pd(name="island_pd_N3"):
                              "partial_dry": True})
 
 
+
+def case_conv_tc1(name="conv_tc1_N3"):
+    """The reference's own convergence test (Testcase 1): manufactured
+    solution, Dirichlet boundary states from the exact solution, its source
+    term; initial state and bathymetry from the reference's set-up."""
+    N = 3
+    params = host.Params(N=N, CFL=0.4, T=0.1, NumFlux=0, rkOrder=4, rkSSP=0, Testcase=1)
+    out = run_ref.run(name, params, cartesian=(0.0, 2.0, 0.0, 2.0, 8, 8, 0, 0))
+    save(name, params, out, {"mesh": "Cartesian 8x8 on [0,2]^2, Dirichlet (exact) boundaries",
+                             "state": "Testcase 1 manufactured solution"})
+
+
 CASES = {
     "periodic_nf0_N3": lambda: case_periodic(0, "periodic_nf0_N3"),
     "periodic_nf3_N3": lambda: case_periodic(3, "periodic_nf3_N3"),
@@ -179,6 +191,7 @@ CASES = {
     "periodic_pp_N3": lambda: case_positivity(),
     "walls_ssp3_N2": lambda: case_ssp_walls(),
     "island_pd_N3": lambda: case_island_pd(),
+    "conv_tc1_N3": lambda: case_conv_tc1(),
 }
 
 

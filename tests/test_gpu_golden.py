@@ -33,12 +33,13 @@ def test_engine_matches_reference_run(name):
         assert err <= 1e-12, (name, v, err)
 
 
-@pytest.mark.parametrize("name", [n for n in fixtures.names() if "_av_" not in n])
+@pytest.mark.parametrize("name", [n for n in fixtures.names() if "_av_" not in n and not n.startswith("conv_")])
 def test_plain_path_is_bitwise_equal_to_reference(name):
     """Built without FMA contraction, the engine performs the reference's
     operations in the reference's order: the plain path (no shock sensor,
-    whose log10/sin come from different math libraries) reproduces the
-    reference's state bit for bit."""
+    whose log10/sin come from different math libraries, and not the
+    manufactured-solution case, whose boundary states and source use
+    sin/cos) reproduces the reference's state bit for bit."""
     prob, q_ref, _ = fixtures.load(name)
     s = Solver(prob)
     try:
