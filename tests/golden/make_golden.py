@@ -204,6 +204,9 @@ DROPIN_CASES = {
     "dropin_tc20_nf0": dict(N=3, T=0.02, NumFlux=0, Testcase=20, cart=(-5.0, 5.0, -5.0, 5.0, 20, 20, 0, 0)),
     "dropin_tc20_nf3_ssp": dict(N=4, T=0.02, NumFlux=3, Testcase=20, rkOrder=3, rkSSP=1,
                                 cart=(-5.0, 5.0, -5.0, 5.0, 12, 10, 0, 0)),
+    # Testcase 1: manufactured solution; its errors against the exact
+    # solution are compared to a relative 1e-6 (sin/cos of two math libraries)
+    "dropin_tc1_conv": dict(N=3, T=0.1, NumFlux=0, Testcase=1, cart=(0.0, 2.0, 0.0, 2.0, 8, 8, 0, 0), rtol=1e-6),
 }
 
 

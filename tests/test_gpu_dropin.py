@@ -5,11 +5,13 @@ but its deviceclass) compiled where they lie and linked against
 libesdg_b200.so through include/dropin/deviceclass.h (built by
 `oracle/build_ref.sh dropin` in a container that has the reference tree;
 the binary travels with the repository, the reference tree does not).  Run
-on a native test case (Testcase 20, Cartesian dam break, solid walls), its
+on native test cases (Testcase 20, Cartesian dam break, solid walls), its
 printed end-of-run diagnostics -- L2 and Linf errors, mass and entropy
 changes, printed with 17 significant digits (main.cpp:77) -- must equal,
 character for character, those of the reference program itself recorded in
-tests/golden/dropin_*.json.
+tests/golden/dropin_*.json; on its convergence test (Testcase 1, errors
+against the exact solution) within a relative 1e-6, as the boundary states
+and the source use sin/cos.
 """
 import glob
 import json
@@ -41,4 +43,13 @@ def test_reference_driver_on_engine_prints_reference_results(case, tmp_path):
                        text=True, timeout=300)
     assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
     got = diag_lines(p.stdout)
-    assert got == rec["diagnostics"], (got, rec["diagnostics"])
+    rtol = rec["spec"].get("rtol")
+    if rtol is None:
+        assert got == rec["diagnostics"], (got, rec["diagnostics"])
+    else:  # printed values whose last digits depend on the math library
+        assert len(got) == len(rec["diagnostics"]) > 0
+        for g, r in zip(got, rec["diagnostics"]):
+            gk, gv = g.rsplit(" ", 1)
+            rk, rv = r.rsplit(" ", 1)
+            assert gk == rk
+            assert abs(float(gv) - float(rv)) <= rtol * abs(float(rv)) + 1e-300, (g, r)
