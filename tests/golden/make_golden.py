@@ -207,12 +207,18 @@ DROPIN_CASES = {
     # Testcase 1: manufactured solution; its errors against the exact
     # solution are compared to a relative 1e-6 (sin/cos of two math libraries)
     "dropin_tc1_conv": dict(N=3, T=0.1, NumFlux=0, Testcase=1, cart=(0.0, 2.0, 0.0, 2.0, 8, 8, 0, 0), rtol=1e-6),
+    # Testcase 5: dry lake + lake at rest (h = max(0, 0.4 - b)), with the
+    # partial-dry treatment and the positivity limiter, solid walls
+    "dropin_tc5_pd": dict(N=3, T=0.05, NumFlux=0, Testcase=5, cart=(0.0, 1.0, 0.0, 1.0, 8, 8, 0, 0),
+                          PositivityPreserving=1, PosPresTOL=1e-3, PartialDryTreatment=1),
 }
 
 
 def dropin_params(spec):
     p = host.Params(N=spec["N"], CFL=0.4, T=spec["T"], NumFlux=spec["NumFlux"], Testcase=spec["Testcase"],
-                    rkOrder=spec.get("rkOrder", 4), rkSSP=spec.get("rkSSP", 0))
+                    rkOrder=spec.get("rkOrder", 4), rkSSP=spec.get("rkSSP", 0),
+                    PositivityPreserving=spec.get("PositivityPreserving", 0),
+                    PosPresTOL=spec.get("PosPresTOL", 1e-4), PartialDryTreatment=spec.get("PartialDryTreatment", 0))
     return p
 
 
