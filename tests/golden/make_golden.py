@@ -211,6 +211,12 @@ DROPIN_CASES = {
     # partial-dry treatment and the positivity limiter, solid walls
     "dropin_tc5_pd": dict(N=3, T=0.05, NumFlux=0, Testcase=5, cart=(0.0, 1.0, 0.0, 1.0, 8, 8, 0, 0),
                           PositivityPreserving=1, PosPresTOL=1e-3, PartialDryTreatment=1),
+    # the reference's lake-at-rest cases on solid walls: a bump on nine
+    # elements of a 20x20 grid (Testcase 2), a smooth bottom (4), no bottom (7)
+    "dropin_tc2_wb": dict(N=3, T=0.05, NumFlux=0, Testcase=2, cart=(0.0, 20.0, 0.0, 20.0, 20, 20, 0, 0)),
+    "dropin_tc4_wb_nf3": dict(N=4, T=0.05, NumFlux=3, Testcase=4, cart=(0.0, 6.0, 0.0, 6.0, 8, 8, 0, 0)),
+    "dropin_tc7_ssp": dict(N=2, T=0.05, NumFlux=0, Testcase=7, rkOrder=3, rkSSP=1,
+                           cart=(0.0, 1.0, 0.0, 1.0, 6, 6, 0, 0)),
 }
 
 
