@@ -217,6 +217,11 @@ DROPIN_CASES = {
     "dropin_tc4_wb_nf3": dict(N=4, T=0.05, NumFlux=3, Testcase=4, cart=(0.0, 6.0, 0.0, 6.0, 8, 8, 0, 0)),
     "dropin_tc7_ssp": dict(N=2, T=0.05, NumFlux=0, Testcase=7, rkOrder=3, rkSSP=1,
                            cart=(0.0, 1.0, 0.0, 1.0, 6, 6, 0, 0)),
+    # dam break with the shock sensor and artificial viscosity (its log10 / sin
+    # come from different math libraries: relative 1e-9)
+    "dropin_tc20_av": dict(N=3, T=0.02, NumFlux=0, Testcase=20, cart=(-5.0, 5.0, -5.0, 5.0, 16, 16, 0, 0),
+                           ArtificialViscosity=1, epsilon_0=0.5, sigma_min=-6.0, sigma_max=-2.0, rtol=1e-9,
+                           atol=1e-10),
 }
 
 
@@ -224,7 +229,9 @@ def dropin_params(spec):
     p = host.Params(N=spec["N"], CFL=0.4, T=spec["T"], NumFlux=spec["NumFlux"], Testcase=spec["Testcase"],
                     rkOrder=spec.get("rkOrder", 4), rkSSP=spec.get("rkSSP", 0),
                     PositivityPreserving=spec.get("PositivityPreserving", 0),
-                    PosPresTOL=spec.get("PosPresTOL", 1e-4), PartialDryTreatment=spec.get("PartialDryTreatment", 0))
+                    PosPresTOL=spec.get("PosPresTOL", 1e-4), PartialDryTreatment=spec.get("PartialDryTreatment", 0),
+                    ArtificialViscosity=spec.get("ArtificialViscosity", 0), epsilon_0=spec.get("epsilon_0", 0.1),
+                    sigma_min=spec.get("sigma_min", -16.0), sigma_max=spec.get("sigma_max", -12.0))
     return p
 
 

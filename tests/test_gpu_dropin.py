@@ -11,7 +11,9 @@ changes, printed with 17 significant digits (main.cpp:77) -- must equal,
 character for character, those of the reference program itself recorded in
 tests/golden/dropin_*.json; on its convergence test (Testcase 1, errors
 against the exact solution) within a relative 1e-6, as the boundary states
-and the source use sin/cos.
+and the source use sin/cos, and on a dam break with artificial viscosity
+within a relative 1e-9 (absolute 1e-10 for the round-off-level mass change
+and transverse error), as the shock sensor uses log10 and sin.
 """
 import glob
 import json
@@ -43,7 +45,7 @@ def test_reference_driver_on_engine_prints_reference_results(case, tmp_path):
                        text=True, timeout=300)
     assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
     got = diag_lines(p.stdout)
-    rtol = rec["spec"].get("rtol")
+    rtol, atol = rec["spec"].get("rtol"), rec["spec"].get("atol", 0.0)
     if rtol is None:
         assert got == rec["diagnostics"], (got, rec["diagnostics"])
     else:  # printed values whose last digits depend on the math library
@@ -52,4 +54,4 @@ def test_reference_driver_on_engine_prints_reference_results(case, tmp_path):
             gk, gv = g.rsplit(" ", 1)
             rk, rv = r.rsplit(" ", 1)
             assert gk == rk
-            assert abs(float(gv) - float(rv)) <= rtol * abs(float(rv)) + 1e-300, (g, r)
+            assert abs(float(gv) - float(rv)) <= rtol * abs(float(rv)) + atol, (g, r)
