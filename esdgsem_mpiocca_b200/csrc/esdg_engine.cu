@@ -1086,6 +1086,7 @@ class Engine {
             *face_ms += a;
             *elem_ms += b;
         }
+        stage_tfrac = 0.0;
         k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
         ++launches;
     }
@@ -1125,6 +1126,7 @@ class Engine {
 
     template <int NGL>
     void launch_rhs() {
+        stage_tfrac = 0.0;  // one RHS at the state's own time
         if (AV) {
             // the step-start sensor (shock_stage=1 recomputes it from q)
             launch_stage<NGL>(2, 0.0, 0.0, 0.0, false, true);
