@@ -134,3 +134,33 @@ def test_okada_matches_reference_routine():
     assert (ref != 0).sum() > 1000
     np.testing.assert_array_equal(mine != 0, ref != 0)
     assert np.abs(mine - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_oracle_reproduces_reference_errors_on_testcase1():
+    """Testcase 1: the reference prints its errors against the exact
+    solution; the oracle's final state gives the same Linf errors."""
+    import json
+    import re
+    from esdgsem_mpiocca_b200 import problems
+    prob, q_ref, z = fixtures.load("conv_tc1_N3")
+    out = OracleProblem(prob).run(T=prob.params.T, max_steps=0)
+    tail = json.loads(bytes(z["meta"]).decode())["reference_stdout_tail"]
+    printed = [float(v) for v in re.findall(r"LinfError\[\d\] is: ([0-9.eE+-]+)", tail)]
+    assert len(printed) == 3
+    d = np.abs(out["q"] - problems.conv_exact(prob, out["t"])).reshape(prob.K, 3, -1)
+    for v in range(3):
+        assert abs(d[:, v].max() - printed[v]) <= 1e-9 * printed[v], (v, d[:, v].max(), printed[v])
+
+
+def test_oracle_converges_at_order_on_testcase1():
+    """The manufactured solution's L2 error in h falls at order N+1."""
+    from esdgsem_mpiocca_b200 import problems
+    errs = []
+    for nel in (4, 8):
+        pr = problems.conv_test(N=3, nel=nel, T=0.1, CFL=0.2)
+        out = OracleProblem(pr).run(T=0.1, max_steps=0)
+        d = (out["q"] - problems.conv_exact(pr, out["t"])).reshape(pr.K, 3, -1)
+        w = np.outer(pr.basis.wGL, pr.basis.wGL).reshape(-1)
+        J = 1.0 / pr.mesh.Jinv.reshape(pr.K, -1)
+        errs.append(float(np.sqrt(((d[:, 0] ** 2) * w * J).sum())))
+    assert np.log2(errs[0] / errs[1]) >= 3.5, errs
