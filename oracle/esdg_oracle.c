@@ -3,7 +3,7 @@
  *
  * Plain-C, single-threaded (optionally OpenMP over elements/faces) restatement
  * of the ESDGSEM_MPIOCCA per-step kernels and of deviceclass::DGtimeloop.
- * It is the checker that the CUDA engine is compared with; nothing in the
+ * It is what the CUDA engine's results are compared with; nothing in the
  * engine links or calls it.  Only tests/, __graft_entry__.smoke() and the
  * cpu_baseline / reference legs of bench.py load it.
  *

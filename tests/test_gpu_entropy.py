@@ -1,5 +1,4 @@
-"""Entropy behaviour of the engine's scheme (the north star's third
-property): with the interface dissipation switched off (ES=0) the
+"""Entropy behaviour of the engine's scheme: with the interface dissipation switched off (ES=0) the
 semi-discrete scheme conserves the total entropy
     S = sum_e sum_ij J w_i w_j ( h (u^2 + v^2) / 2 + g h^2 / 2 + g h b )
 to round-off, i.e. the entropy variables w = (g (h + b) - (u^2 + v^2) / 2,

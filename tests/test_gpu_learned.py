@@ -1,5 +1,5 @@
 """The trained indicator networks (esdgsem_mpiocca_b200/weights) in the
-solver, judged by the modal sensor on seeds the training never saw:
+solver, measured against the modal sensor on seeds the training never saw:
 
 * flag agreement: on snapshots of a plain-sensor run, the viscosity the
   learned indicator assigns (network where confident, modal sensor
