@@ -35,6 +35,8 @@ def _declare(lib):
         "esdg_copy_q_to_host": (_I, [_VP, _PD]),
         "esdg_copy_q_from_host": (_I, [_VP, _PD]),
         "esdg_copy_visc_to_host": (_I, [_VP, _PD]),
+        "esdg_copy_arrival_times": (_I, [_VP, _PD]),
+        "esdg_copy_maximum_elevation": (_I, [_VP, _PD]),
         "esdg_bytes_allocated": (ctypes.c_longlong, [_VP]),
         "esdg_kernel_launches": (ctypes.c_longlong, [_VP]),
         "esdg_free_occa_vars": (_I, [_VP, _I, _I, _I]),

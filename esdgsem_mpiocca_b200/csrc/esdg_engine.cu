@@ -30,6 +30,7 @@
 #include "esdg_tma.cuh"
 #include "esdg_rows.cuh"
 #include "esdg_indicator.cuh"
+#include "esdg_analysis.cuh"
 #include "esdg_setup.hpp"
 
 namespace esdg {
@@ -126,6 +127,9 @@ class Engine {
     double *SGX = nullptr, *SGY = nullptr, *SPV = nullptr, *GX = nullptr, *GY = nullptr, *VP = nullptr;
     int *EdgeData = nullptr;
     int4 *ftab = nullptr, *side = nullptr;
+    // analysis outputs per node (initDeviceVariables' CalcArrivalTimes and
+    // CalcMaximumElevation; null when off)
+    double *arrival = nullptr, *max_elev = nullptr;
     DevState* st = nullptr;
     DevState* st_host = nullptr;  // pinned mirror for polling
     int* elem_inst = nullptr;     // null: one instance
@@ -208,6 +212,7 @@ class Engine {
         indX = nullptr; ind_seta = ind_y = nullptr; ind_energy = nullptr; ind_ok = nullptr;
         indicator = 0;
         dry = nullptr; DcFD = DupFD = DdnFD = nullptr; pd_copied = false;
+        arrival = max_elev = nullptr;
         inited = copied = built = false;
     }
 
@@ -229,7 +234,7 @@ class Engine {
 
     int init(int N_, int K_, int F_, int rank_, int rkSSP_, int ES_, int Testcase_, double eps0_, double smax,
              double smin, double tol, double geomface, double g_, int PP_, int AV_, int DiscBottom_, double h0_,
-             int PartialDry_, int Friction_) {
+             int PartialDry_, int Friction_, int ArrivalTimes_ = 0, int MaxElevation_ = 0) {
         if (inited) release();
         if (N_ < 1 || N_ > 7) return fail(ESDG_E_UNSUPPORTED, "N must be in 1..7");
         if (K_ <= 0 || F_ <= 0) return fail(ESDG_E_ARG, "Nelem and Nfaces must be positive");
@@ -266,6 +271,11 @@ class Engine {
                 (r = alloc(&GX, nn * 2)) || (r = alloc(&GY, nn * 2)) || (r = alloc(&VP, (size_t)K)))
                 return r;
         }
+        if (ArrivalTimes_) {
+            if ((r = alloc(&arrival, nn))) return r;
+            k_fill_f64<<<(unsigned)((nn + 255) / 256), 256>>>(arrival, (long)nn, 1000.0);
+        }
+        if (MaxElevation_ && (r = alloc(&max_elev, nn))) return r;  // from 0, as the reference's calloc
         if ((r = alloc(&st, (size_t)I))) return r;
         cudaError_t e = cudaMallocHost(&st_host, sizeof(DevState));
         if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
@@ -843,6 +853,17 @@ class Engine {
         return gB[s];
     }
 
+    // Arrival times / maximum elevation with the step's new time
+    // (src/deviceclass.cpp:1130-1141).
+    template <int NGL>
+    void launch_analysis() {
+        if (!arrival && !max_elev) return;
+        const long nodes = (long)K * NGL * NGL;
+        k_analysis<NGL * NGL><<<(unsigned)((nodes + 255) / 256), 256, 0, stream>>>(nodes, q, B, st, h0, arrival,
+                                                                                   max_elev);
+        ++launches;
+    }
+
     template <int NGL>
     void launch_step() {
         if (AV) launch_indicator<NGL>(1);
@@ -859,6 +880,7 @@ class Engine {
         stage_tfrac = 0.0;
         k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
         ++launches;
+        launch_analysis<NGL>();
     }
 
 #define ESDG_DISPATCH(NGLV, CALL)                 \
@@ -1089,6 +1111,7 @@ class Engine {
         stage_tfrac = 0.0;
         k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
         ++launches;
+        launch_analysis<NGL>();
     }
 
     int profile_steps(int nsteps, double* face_ms, double* elem_ms) {
@@ -1216,10 +1239,10 @@ int esdg_init_device_variables(esdg_deviceclass* d, int N, int Nelem, int Nfaces
                                int CreateTimeSeries, int CalcMaximumElevation) {
     ESDG_GUARD(d);
     (void)NEpad; (void)NEsurfpad; (void)Nedgepad; (void)NAvgPad;  // launch shapes are chosen per ngl
-    (void)CalcArrivalTimes; (void)CreateTimeSeries; (void)CalcMaximumElevation;  // analysis outputs: not rebuilt
+    (void)CreateTimeSeries;  // gauge time series are written by the reference's plot checkpoints: not rebuilt
     return d->eng.init(N, Nelem, Nfaces, rank, rkSSP, ES, Testcase, epsilon_0, sigma_max, sigma_min, PosPresTOL,
                        geomface, g_const, PositivityPreserving, ArtificialViscosity, DiscBottom, h_0, PartialDry,
-                       FrictionTerms);
+                       FrictionTerms, CalcArrivalTimes, CalcMaximumElevation);
 }
 
 int esdg_copy_device_variables(esdg_deviceclass* d, int PositivityPreserving, int Nelem, const double* GLw,
@@ -1297,6 +1320,27 @@ int esdg_copy_visc_to_host(esdg_deviceclass* d, double* visc) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
     if (e != cudaSuccess) return E.cuda_fail(e, "copy_visc_to_host");
     return ESDG_OK;
+}
+
+static int copy_analysis(esdg_deviceclass* d, const double* src, double* out, const char* what) {
+    esdg::Engine& E = d->eng;
+    if (!E.inited || !src || !out)
+        return E.fail(ESDG_E_ARG, std::string(what) + ": not enabled at initDeviceVariables, or null");
+    cudaError_t e = cudaMemcpyAsync(out, src, (size_t)E.K * E.ngl * E.ngl * sizeof(double), cudaMemcpyDeviceToHost,
+                                    E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    if (e != cudaSuccess) return E.cuda_fail(e, what);
+    return ESDG_OK;
+}
+
+int esdg_copy_arrival_times(esdg_deviceclass* d, double* arrival_times) {
+    ESDG_GUARD(d);
+    return copy_analysis(d, d->eng.arrival, arrival_times, "copy_arrival_times");
+}
+
+int esdg_copy_maximum_elevation(esdg_deviceclass* d, double* maximum_elevation) {
+    ESDG_GUARD(d);
+    return copy_analysis(d, d->eng.max_elev, maximum_elevation, "copy_maximum_elevation");
 }
 
 long long esdg_bytes_allocated(const esdg_deviceclass* d) { return d ? (long long)d->eng.bytes : -1; }

@@ -134,6 +134,16 @@ class DeviceClass:
         self._ok(self._L.esdg_copy_visc_to_host(self.h, pd(v)))
         return v
 
+    def copy_arrival_times(self, nodes: int):
+        a = np.zeros(nodes)
+        self._ok(self._L.esdg_copy_arrival_times(self.h, pd(a)))
+        return a
+
+    def copy_maximum_elevation(self, nodes: int):
+        a = np.zeros(nodes)
+        self._ok(self._L.esdg_copy_maximum_elevation(self.h, pd(a)))
+        return a
+
     def set_stream(self, stream_ptr: int | None):
         self._ok(self._L.esdg_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
 
@@ -214,8 +224,8 @@ class Solver:
         self.dc = DeviceClass(0, device_id)
         self.dc.initDeviceVariables(p.N, m.K, m.F, 0, p.rkSSP, p.NEpad, p.NEsurfpad, p.Nedgepad, p.NavgPad, p.ES,
                                     p.Testcase, p.epsilon_0, p.sigma_max, p.sigma_min, p.PosPresTOL, bs.geomface,
-                                    p.g_const, p.PositivityPreserving, p.ArtificialViscosity, p.DiscBottom, 0.0,
-                                    p.PartialDryTreatment, 0, 0, 0, 0)
+                                    p.g_const, p.PositivityPreserving, p.ArtificialViscosity, p.DiscBottom, p.h_0,
+                                    p.PartialDryTreatment, 0, p.ArrivalTimings, 0, p.maximumElevation)
         zeros = np.zeros_like(prob.q0)
         self.dc.copyDeviceVariables(p.PositivityPreserving, m.K, bs.wGL, m.nx, m.ny, m.scal, m.y_xi, m.y_eta, m.x_xi,
                                     m.x_eta, prob.b, prob.Bx, prob.By, bs.D, bs.Dstrong, bs.Dhat, m.Jinv, m.x, m.y,
@@ -241,6 +251,12 @@ class Solver:
 
     def rhs(self):
         return self.dc.compute_rhs(self.prob.K, self.prob.ngl, bool(self.prob.params.ArtificialViscosity))
+
+    def arrival_times(self):
+        return self.dc.copy_arrival_times(self.prob.K * self.prob.ngl ** 2)
+
+    def maximum_elevation(self):
+        return self.dc.copy_maximum_elevation(self.prob.K * self.prob.ngl ** 2)
 
     def close(self):
         self.dc.close()

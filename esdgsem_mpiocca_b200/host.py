@@ -204,6 +204,11 @@ class Params:
     DiscBottom: int = 0
     PartialDryTreatment: int = 0
     MaxSteps: int = 0
+    # analysis outputs (input.dat lines ArrivalTimings / maximumElevation)
+    # and the still-water level h_0 they are measured from
+    ArrivalTimings: int = 0
+    maximumElevation: int = 0
+    h_0: float = 0.0
 
 
 @dataclass

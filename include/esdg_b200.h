@@ -36,7 +36,12 @@ typedef struct esdg_deviceclass esdg_deviceclass;
 int esdg_deviceclass_create(int rank, int device_id, esdg_deviceclass** out);
 
 /* deviceclass::initDeviceVariables -- include/deviceclass.h:32-57,
- * src/deviceclass.cpp:108-345 (constants + device allocations). */
+ * src/deviceclass.cpp:108-345 (constants + device allocations).
+ * CalcArrivalTimes / CalcMaximumElevation allocate the per-node analysis
+ * outputs that every time step updates (read them with
+ * esdg_copy_arrival_times / esdg_copy_maximum_elevation); h_0 is the
+ * still-water level they are measured from.  CreateTimeSeries is accepted
+ * and ignored. */
 int esdg_init_device_variables(esdg_deviceclass* d, int N, int Nelem, int Nfaces, int rank, int rkSSP, int NEpad,
                                int NEsurfpad, int Nedgepad, int NAvgPad, int ES, int Testcase, double epsilon_0,
                                double sigma_max, double sigma_min, double PosPresTOL, double geomface,
@@ -129,6 +134,15 @@ int esdg_profile_steps(esdg_deviceclass* d, int nsteps, double* face_ms, double*
 
 /* Element viscosity of the last step (AV only) [K]. */
 int esdg_copy_visc_to_host(esdg_deviceclass* d, double* visc);
+
+/* The analysis outputs as DGtimeloop reads them back at its end
+ * (src/deviceclass.cpp:1296-1309), per node [K*n*n]: the arrival time
+ * (okl/Analysis/ArrivalTimes.okl; 1000.0 where the surface never departed
+ * from h_0 by more than 5e-5) and the maximum of h + b - h_0 since the
+ * start, from 0 (okl/Analysis/MaximumElevation.okl).  ESDG_E_ARG unless
+ * enabled at esdg_init_device_variables. */
+int esdg_copy_arrival_times(esdg_deviceclass* d, double* arrival_times);
+int esdg_copy_maximum_elevation(esdg_deviceclass* d, double* maximum_elevation);
 
 /* Number of kernel launches issued by the engine since creation (graph
  * replays count the kernels inside the graph). */

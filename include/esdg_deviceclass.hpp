@@ -127,6 +127,12 @@ class deviceclass {
     }
 
     // engine extras
+    // the per-node analysis outputs of src/deviceclass.cpp:1296-1309, which
+    // the reference writes as Tecplot files at the end of DGtimeloop
+    void copyArrivalTimes(double* out) { check(esdg_copy_arrival_times(h_, out), h_, "copyArrivalTimes"); }
+    void copyMaximumElevation(double* out) {
+        check(esdg_copy_maximum_elevation(h_, out), h_, "copyMaximumElevation");
+    }
     esdg_deviceclass* handle() const { return h_; }
     double last_time() const { return last_t_; }
     int last_steps() const { return last_steps_; }

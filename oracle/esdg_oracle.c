@@ -895,6 +895,26 @@ static void volume_partial_dry(const oconst* c, int K, const double* Jac, const 
     }
 }
 
+/* Analysis outputs after a step, with the new time t (called after t += dt
+ * at src/deviceclass.cpp:1130-1141): okl/Analysis/ArrivalTimes.okl:16-62
+ * (first t at which |h + b - h_zero| exceeds 5e-5 while the entry is still
+ * the sentinel 1000.0) and okl/Analysis/MaximumElevation.okl:16-55 (running
+ * std::max of h + b - h_zero). */
+static void analysis(int K, int n2, double t, double h_zero, const double* Q, const double* B, double* AT,
+                     double* ME) {
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < K; ++e)
+        for (int id = 0; id < n2; ++id) {
+            const long x = (long)e * n2 + id;
+            const double h = Q[(long)e * n2 * NEQ + id];
+            if (AT && AT[x] == 1000.0 && fabs((h + B[x]) - h_zero) > 0.00005) AT[x] = t;
+            if (ME) {
+                const double fs = h + B[x] - h_zero;
+                ME[x] = ME[x] < fs ? fs : ME[x];
+            }
+        }
+}
+
 /* ========================================================================= */
 /* Public entry points                                                        */
 /* ========================================================================= */
@@ -910,6 +930,11 @@ typedef struct {
     /* Testcase 1 (manufactured solution): nodal coordinates */
     const double *X, *Y;
     int Testcase;
+    /* analysis outputs updated after every step of oracle_timeloop (NULL:
+     * off; the caller fills them with 1000.0 and 0) and the still-water
+     * level they are measured from */
+    double *ArrivalTimes, *MaxElevation;
+    double h0;
 } oracle_geom;
 
 /* One right-hand-side evaluation Qt = L(q) (no AV), as the stage body of
@@ -1059,6 +1084,8 @@ int oracle_timeloop(int N, int K, int F, const oracle_geom* G, double* q, double
         }
         t += dt;
         ++steps;
+        if (G->ArrivalTimes || G->MaxElevation)
+            analysis(K, n2, t, G->h0, q, G->B, G->ArrivalTimes, G->MaxElevation);
     }
     if (visc_out && AV) memcpy(visc_out, VP, (size_t)K * sizeof(double));
     if (t_out) *t_out = t;

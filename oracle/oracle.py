@@ -25,7 +25,8 @@ class _Geom(ctypes.Structure):
                                    "Dstrong", "Dhat", "VdmInv", "GLw", "EleSizes")] + \
                [(n, _PI) for n in ("EdgeData", "EdgeReversed", "ElemToEdge", "MasterSlave", "Orientation")] + \
                [(n, _PD) for n in ("DcFD", "DfFD", "DbFD")] + [("PD", ctypes.c_int)] + \
-               [(n, _PD) for n in ("X", "Y")] + [("Testcase", ctypes.c_int)]
+               [(n, _PD) for n in ("X", "Y")] + [("Testcase", ctypes.c_int)] + \
+               [(n, _PD) for n in ("ArrivalTimes", "MaxElevation")] + [("h0", ctypes.c_double)]
 
 
 _LIB = None
@@ -81,7 +82,8 @@ class OracleProblem:
         self._xy = [np.ascontiguousarray(a, dtype=np.float64) for a in (m.x, m.y)]
         self.g = _Geom(**{k: _p(v) for k, v in self._arrs.items()}, **{k: _p(v, _PI) for k, v in self._ints.items()},
                        DcFD=_p(self._fd[0]), DfFD=_p(self._fd[1]), DbFD=_p(self._fd[2]), PD=pd,
-                       X=_p(self._xy[0]), Y=_p(self._xy[1]), Testcase=int(prob.params.Testcase))
+                       X=_p(self._xy[0]), Y=_p(self._xy[1]), Testcase=int(prob.params.Testcase),
+                       h0=float(getattr(prob.params, "h_0", 0.0)))
 
     def rhs(self, q):
         p = self.prob.params
@@ -108,14 +110,24 @@ class OracleProblem:
         dts = np.zeros(max(ms, 1)) if (log_dt and ms > 0) else None
         visc = np.zeros(self.prob.K) if p.ArtificialViscosity else None
         A, B, C = (np.ascontiguousarray(v, dtype=np.float64) for v in (self.prob.rkA, self.prob.rkB, self.prob.rkC))
+        nodes = self.prob.K * (p.N + 1) ** 2
+        at = np.full(nodes, 1000.0) if getattr(p, "ArrivalTimings", 0) else None
+        me = np.zeros(nodes) if getattr(p, "maximumElevation", 0) else None
+        self.g.ArrivalTimes = None if at is None else _p(at)
+        self.g.MaxElevation = None if me is None else _p(me)
         rc = lib().oracle_timeloop(p.N, self.prob.K, self.prob.F, ctypes.byref(self.g), _p(q), p.g_const,
                                    p.PosPresTOL, p.ES, p.NumFlux, len(A), _p(A), _p(B), _p(C), p.rkSSP,
                                    p.ArtificialViscosity, p.PositivityPreserving, p.epsilon_0, p.sigma_min,
                                    p.sigma_max, self.prob.minEleSize, p.CFL, p.DFL, T, ms, ctypes.byref(t),
                                    ctypes.byref(s), None if dts is None else _p(dts),
                                    None if visc is None else _p(visc))
+        self.g.ArrivalTimes = self.g.MaxElevation = None
         assert rc == 0
         out = {"q": q, "t": t.value, "steps": s.value}
+        if at is not None:
+            out["ArrivalTimings"] = at
+        if me is not None:
+            out["MaximumElevation"] = me
         if dts is not None:
             out["dt"] = dts[: s.value]
         if visc is not None:

@@ -49,9 +49,12 @@ def build():
     return EXE
 
 
-def seq_names(pp: int, pd: int = 0):
-    # copyPartialDryData (main.cpp:938-941) follows copyDeviceVariables
-    return SEQ_BEFORE_GLW + (["GLw"] if pp else []) + SEQ_AFTER_GLW + (["DcFD", "DfFD", "DbFD"] if pd else [])
+def seq_names(pp: int, pd: int = 0, at: int = 0, me: int = 0):
+    # initDeviceVariables first fills the arrival-time and maximum-elevation
+    # buffers (src/deviceclass.cpp:324-341); copyPartialDryData
+    # (main.cpp:938-941) follows copyDeviceVariables
+    return ((["ArrivalTimings0"] if at else []) + (["MaximumElevation0"] if me else []) + SEQ_BEFORE_GLW +
+            (["GLw"] if pp else []) + SEQ_AFTER_GLW + (["DcFD", "DfFD", "DbFD"] if pd else []))
 
 
 def write_input(path, params, mesh_file="none", cartesian=1):
@@ -66,7 +69,8 @@ def write_input(path, params, mesh_file="none", cartesian=1):
             "NavgPad": params.NavgPad, "KernelVersionFD": 99, "KernelVersionSTD": 99, "DiscBottom": 0,
             "ReadInBottom": 0, "PartialDryTreatment": 0, "FrictionTerms": 0, "ConvertToKM": 0, "ArrivalTimings": 0,
             "createTimeSeries": 0, "maximumElevation": 0}
-    vals["PartialDryTreatment"] = int(getattr(params, "PartialDryTreatment", 0))
+    for k in ("PartialDryTreatment", "ArrivalTimings", "maximumElevation"):
+        vals[k] = int(getattr(params, k, 0))
     with open(path, "w") as f:
         for k in INPUT_KEYS:
             f.write(f"{k}={vals[k]}\n")
@@ -99,7 +103,8 @@ def run(tag, params, cartesian=None, mesh_file=None, inject=None, mode="Serial",
         write_cartesian(os.path.join(rd, "Cartesian.dat"), *cartesian)
     else:
         write_input(os.path.join(rd, "input.dat"), params, mesh_file, 0)
-    names = seq_names(params.PositivityPreserving, int(getattr(params, "PartialDryTreatment", 0)))
+    names = seq_names(params.PositivityPreserving, int(getattr(params, "PartialDryTreatment", 0)),
+                      int(getattr(params, "ArrivalTimings", 0)), int(getattr(params, "maximumElevation", 0)))
     for k, v in (inject or {}).items():
         np.ascontiguousarray(v, dtype=np.float64).tofile(os.path.join(rd, "inject", f"from_{names.index(k):03d}.bin"))
     env = dict(os.environ)
@@ -127,4 +132,10 @@ def run(tag, params, cartesian=None, mesh_file=None, inject=None, mode="Serial",
         out[nm] = np.fromfile(fn, dtype=np.int32 if nm in INT_ARRAYS else np.float64)
     qmem = mem_of_seq[names.index("q")]
     out["q_final"] = np.fromfile(os.path.join(rd, "dump", f"to_{qmem:03d}.bin"), dtype=np.float64)
+    # the analysis buffers as DGtimeloop reads them back at its end
+    # (src/deviceclass.cpp:1296-1309)
+    for nm in ("ArrivalTimings", "MaximumElevation"):
+        if nm + "0" in names:
+            mem = mem_of_seq[names.index(nm + "0")]
+            out[nm] = np.fromfile(os.path.join(rd, "dump", f"to_{mem:03d}.bin"), dtype=np.float64)
     return out

@@ -24,6 +24,8 @@ def load(name):
     z = np.load(os.path.join(HERE, f"{name}.npz"))
     meta = json.loads(bytes(z["meta"]).decode())
     p = host.Params(**meta["params"])
+    if meta.get("reference_h_zero") is not None:  # the h_0 the reference's analysis kernels measured from
+        p.h_0 = float(meta["reference_h_zero"])
     N = p.N
     n2 = (N + 1) ** 2
     K = z["Jinv"].size // n2

@@ -182,6 +182,33 @@ def case_conv_tc1(name="conv_tc1_N3"):
                              "state": "Testcase 1 manufactured solution"})
 
 
+def case_analysis(name="walls_analysis_N3"):
+    """Arrival times and maximum elevation (okl/Analysis/*): a ripple on a
+    lake whose still-water level is 0 (b = -depth), walls.  The reference
+    measures both from its h_0, which main.cpp sets only when it reads a
+    bottom file (main.cpp:370,515); otherwise the value is whatever the
+    stack held, recorded here from the compiled kernel's define (a
+    subnormal in the runs seen, i.e. 0 for these results)."""
+    import glob
+    import re
+    N = 3
+    params = host.Params(N=N, CFL=0.4, T=0.08, NumFlux=0, rkOrder=4, rkSSP=0, ArrivalTimings=1,
+                         maximumElevation=1)
+    m = host.mesh_cartesian(N, 0.0, 1.0, 0.0, 1.0, 12, 12)
+    x, y = m.x, m.y
+    b = -1.0 + 0.3 * np.exp(-((x - 0.6) ** 2 + (y - 0.55) ** 2) / 0.2 ** 2)
+    h = -b + 0.01 * np.exp(-((x - 0.25) ** 2 + (y - 0.3) ** 2) / 0.06 ** 2)
+    basis = host.Basis.build(N)
+    Bx, By = host.bottom_derivatives(m, basis, b)
+    out = run_ref.run(name, params, cartesian=(0.0, 1.0, 0.0, 1.0, 12, 12, 0, 0),
+                      inject={"q": pack_q(h, n2=(N + 1) ** 2), "b": b, "Bx": Bx, "By": By})
+    kc = sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "kcache", "*.cpp")), key=os.path.getmtime)
+    hz = [re.findall(r"#define h_zero \((.*)\)", open(f).read()) for f in kc
+          if "Arrivaltimes" in open(f).read()]
+    save(name, params, out, {"mesh": "Cartesian walls 12x12 on [0,1]^2", "state": "ripple, still water at 0",
+                             "reference_h_zero": hz[-1][0] if hz and hz[-1] else None})
+
+
 CASES = {
     "periodic_nf0_N3": lambda: case_periodic(0, "periodic_nf0_N3"),
     "periodic_nf3_N3": lambda: case_periodic(3, "periodic_nf3_N3"),
@@ -192,6 +219,7 @@ CASES = {
     "walls_ssp3_N2": lambda: case_ssp_walls(),
     "island_pd_N3": lambda: case_island_pd(),
     "conv_tc1_N3": lambda: case_conv_tc1(),
+    "walls_analysis_N3": lambda: case_analysis(),
 }
 
 

@@ -34,6 +34,21 @@ def test_oracle_reproduces_reference_bitwise(name):
     np.testing.assert_array_equal(out["q"], q_ref)
 
 
+def test_oracle_reproduces_reference_analysis_outputs():
+    """Arrival times and maximum elevation (okl/Analysis/*), updated after
+    every step, equal the arrays the reference's DGtimeloop read back at its
+    end, bit for bit; the ripple reached part of the lake and not all of it."""
+    prob, q_ref, z = fixtures.load("walls_analysis_N3")
+    out = OracleProblem(prob).run(T=prob.params.T, max_steps=0)
+    np.testing.assert_array_equal(out["q"], q_ref)
+    np.testing.assert_array_equal(out["ArrivalTimings"], z["ArrivalTimings"])
+    np.testing.assert_array_equal(out["MaximumElevation"], z["MaximumElevation"])
+    at = z["ArrivalTimings"]
+    assert 0 < (at == 1000.0).sum() < at.size
+    assert len(np.unique(at[at < 1000.0])) > 10  # arrivals spread over many steps
+    assert z["MaximumElevation"].max() > 0.005
+
+
 @pytest.mark.parametrize("N", [2, 3, 4])
 def test_basis_matches_reference(N):
     name = {2: "walls_ssp3_N2", 3: "periodic_nf0_N3", 4: "mapped_rot_N4"}[N]
