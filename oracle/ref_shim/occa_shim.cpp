@@ -154,22 +154,57 @@ static std::string read_file(const std::string& path) {
     return ss.str();
 }
 
+static kernel load_kernel(const std::string& so, const std::string& name, const std::string& file) {
+    void* hdl = dlopen(so.c_str(), RTLD_NOW | RTLD_LOCAL);
+    if (!hdl) throw std::runtime_error(std::string("occa shim: dlopen: ") + dlerror());
+    kernel k;
+    k.fn = dlsym(hdl, name.c_str());
+    if (!k.fn) throw std::runtime_error("occa shim: kernel " + name + " not found in " + file);
+    k.name = name;
+    return k;
+}
+
+// Kernels are cached by the hash of their translated source.  Each cached
+// kernel is also entered under an index key made of what the program asks
+// for -- file name, kernel name, mode and defines -- so that a machine
+// without the reference's .okl tree can run the program on kernels built
+// here.  `h_zero` is left out of that key for kernels that do not read it:
+// main.cpp passes an uninitialised h_0 unless it reads a bottom file
+// (main.cpp:370,515), so its value differs from run to run.
+static std::string index_path(const std::string& dir, const std::string& file, const std::string& name, bool omp,
+                              const kernelInfo& info, bool with_h_zero) {
+    std::string key = file + "|" + name + "|" + (omp ? "omp" : "serial") + "|";
+    for (auto& d : info.defines)
+        if (with_h_zero || d.first != "h_zero") key += d.first + "=" + d.second + ";";
+    char stem[64];
+    std::snprintf(stem, sizeof stem, "/i_%016zx.so", std::hash<std::string>{}(key));
+    return dir + stem;
+}
+
 kernel device::buildKernelFromSource(const std::string& file, const std::string& name, const kernelInfo& info) {
     const bool omp = (mode == "OpenMP");
+    const char* cache = env("ESDG_REF_KCACHE");
+    std::string dir = cache ? cache : "kcache";
+    struct stat stt;
+    if (stat(file.c_str(), &stt) != 0) {  // no source here: a kernel built before, by its index key
+        for (bool with_h : {false, true}) {
+            const std::string ip = index_path(dir, file, name, omp, info, with_h);
+            if (stat(ip.c_str(), &stt) == 0) return load_kernel(ip, name, file);
+        }
+        throw std::invalid_argument("occa shim: kernel source not found and no prebuilt kernel: " + file);
+    }
     std::string body = read_file(file);
     std::ostringstream pre;
     pre << "#include <cmath>\n#include <algorithm>\nusing std::max; using std::min;\n"
            "using std::sqrt; using std::fabs; using std::log10; using std::sin; using std::pow;\n";
     for (auto& d : info.defines) pre << "#define " << d.first << " " << d.second << "\n";
-    const std::string code = pre.str() + translate(body, omp);
+    const std::string kbody = translate(body, omp);
+    const std::string code = pre.str() + kbody;
     const size_t h = std::hash<std::string>{}(code + (omp ? "omp" : "serial"));
-    const char* cache = env("ESDG_REF_KCACHE");
-    std::string dir = cache ? cache : "kcache";
     mkdir(dir.c_str(), 0755);
     char stem[64];
     std::snprintf(stem, sizeof stem, "/k_%016zx", h);
     const std::string cpp = dir + stem + ".cpp", so = dir + stem + ".so";
-    struct stat stt;
     if (stat(so.c_str(), &stt) != 0) {
         {
             std::ofstream f(cpp);
@@ -179,13 +214,13 @@ kernel device::buildKernelFromSource(const std::string& file, const std::string&
                                 "-o " + so + ".tmp " + cpp + " && mv " + so + ".tmp " + so;
         if (std::system(cmd.c_str()) != 0) throw std::runtime_error("occa shim: kernel compile failed: " + cpp);
     }
-    void* hdl = dlopen(so.c_str(), RTLD_NOW | RTLD_LOCAL);
-    if (!hdl) throw std::runtime_error(std::string("occa shim: dlopen: ") + dlerror());
-    kernel k;
-    k.fn = dlsym(hdl, name.c_str());
-    if (!k.fn) throw std::runtime_error("occa shim: kernel " + name + " not found in " + file);
-    k.name = name;
-    return k;
+    const bool reads_h_zero = std::regex_search(kbody, std::regex(R"(\bh_zero\b)"));
+    const std::string ip = index_path(dir, file, name, omp, info, reads_h_zero);
+    if (stat(ip.c_str(), &stt) != 0) {
+        const std::string cmd = "cp " + so + " " + ip + ".tmp && mv " + ip + ".tmp " + ip;
+        if (std::system(cmd.c_str()) != 0) throw std::runtime_error("occa shim: kernel index entry failed: " + ip);
+    }
+    return load_kernel(so, name, file);
 }
 
 }  // namespace occa

@@ -10,8 +10,11 @@ bathymetry by the problem's (copyDeviceVariables arguments 7-9 and 16), its
 ESDG_REF_DUMP hook records every copyDeviceVariables argument and the final
 o_q.copyTo(q) of main.cpp:1051.
 
-Only used to generate and check fixtures; needs the reference tree, so it
-runs in the build container, not on the GPU box.
+`run` generates and checks fixtures and needs the reference tree.
+`run_timed` runs the program once without dumps and returns its own timing
+of DGtimeloop; it also runs where the reference tree is absent, as long as
+every kernel the run needs was built before (`warm_kernels` builds them, the
+shim finds them in _ref/kcache by its index).
 """
 from __future__ import annotations
 
@@ -139,3 +142,60 @@ def run(tag, params, cartesian=None, mesh_file=None, inject=None, mode="Serial",
             mem = mem_of_seq[names.index(nm + "0")]
             out[nm] = np.fromfile(os.path.join(rd, "dump", f"to_{mem:03d}.bin"), dtype=np.float64)
     return out
+
+
+def _prepare(rd, params, mesh_file, inject, cartesian=None):
+    if cartesian is not None:
+        write_input(os.path.join(rd, "input.dat"), params, "none", 1)
+        write_cartesian(os.path.join(rd, "Cartesian.dat"), *cartesian)
+    else:
+        write_input(os.path.join(rd, "input.dat"), params, mesh_file, 0)
+    names = seq_names(params.PositivityPreserving, int(getattr(params, "PartialDryTreatment", 0)),
+                      int(getattr(params, "ArrivalTimings", 0)), int(getattr(params, "maximumElevation", 0)))
+    os.makedirs(os.path.join(rd, "inject"), exist_ok=True)
+    for k, v in (inject or {}).items():
+        np.ascontiguousarray(v, dtype=np.float64).tofile(os.path.join(rd, "inject", f"from_{names.index(k):03d}.bin"))
+    if available():
+        for d in ("okl", "meshFiles", "data"):
+            os.symlink(os.path.join(REF, d), os.path.join(rd, d))
+
+
+def run_timed(params, mesh_file, inject=None, threads=None, mode="OpenMP", timeout=900):
+    """One run of the reference program on an absolute mesh path, state and
+    bathymetry injected as in `run`, no dumps.  Returns (seconds, stdout):
+    the time its own timer reports around DGtimeloop (main.cpp:1009-1072,
+    printed as "time taken in seconds")."""
+    import re
+    import tempfile
+    if not os.path.exists(EXE):
+        raise FileNotFoundError(f"reference program not built: {EXE}")
+    rd = tempfile.mkdtemp(prefix="esdg_ref_")
+    try:
+        _prepare(rd, params, mesh_file, inject)
+        env = dict(os.environ)
+        env.pop("ESDG_REF_DUMP", None)
+        env["ESDG_REF_INJECT"] = os.path.join(rd, "inject")
+        env["ESDG_REF_KCACHE"] = os.path.join(HERE, "_ref", "kcache")
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        p = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {EXE} {mode}"], cwd=rd, env=env,
+                           capture_output=True, text=True, timeout=timeout)
+    finally:
+        shutil.rmtree(rd, ignore_errors=True)
+    m = re.search(r"time taken in seconds = ([0-9.eE+-]+)", p.stdout)
+    if p.returncode != 0 or not m:
+        raise RuntimeError(f"reference run failed ({p.returncode}):\n{p.stdout[-2000:]}\n{p.stderr[-2000:]}")
+    return float(m.group(1)), p.stdout
+
+
+def warm_kernels(params, mesh_file, mode="OpenMP"):
+    """Builds (here, from the reference tree) every kernel a run with these
+    parameters loads, so that `run_timed` with the same parameters needs no
+    .okl sources.  The kernels depend on the parameters, not on the mesh:
+    a small mesh does."""
+    if not available():
+        return False
+    if not os.path.exists(EXE):
+        build()
+    run_timed(params, mesh_file, None, threads=2, mode=mode, timeout=600)
+    return True
