@@ -1,6 +1,5 @@
 """The C-ABI library (CPU, no GPU calls): it loads, exports every function
 include/esdg_b200.h declares, and its host set-up entry points behave."""
-import ctypes
 import os
 import re
 import subprocess

@@ -4,7 +4,6 @@ disjoint per-rank sharding of ensemble members (no data-path exchange)."""
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 
