@@ -160,32 +160,43 @@ def _prepare(rd, params, mesh_file, inject, cartesian=None):
             os.symlink(os.path.join(REF, d), os.path.join(rd, d))
 
 
-def run_timed(params, mesh_file, inject=None, threads=None, mode="OpenMP", timeout=900):
+def run_timed(params, mesh_file, inject=None, threads=None, mode="OpenMP", timeout=900, want_q=False):
     """One run of the reference program on an absolute mesh path, state and
-    bathymetry injected as in `run`, no dumps.  Returns (seconds, stdout):
+    bathymetry injected as in `run`.  Returns (seconds, stdout, q_final):
     the time its own timer reports around DGtimeloop (main.cpp:1009-1072,
-    printed as "time taken in seconds")."""
+    printed as "time taken in seconds"), and with want_q the final state
+    (o_q.copyTo at main.cpp:1051, through the dump hook; None otherwise)."""
     import re
     import tempfile
     if not os.path.exists(EXE):
         raise FileNotFoundError(f"reference program not built: {EXE}")
     rd = tempfile.mkdtemp(prefix="esdg_ref_")
+    q_final = None
     try:
         _prepare(rd, params, mesh_file, inject)
         env = dict(os.environ)
         env.pop("ESDG_REF_DUMP", None)
+        if want_q:
+            os.makedirs(os.path.join(rd, "dump"))
+            env["ESDG_REF_DUMP"] = os.path.join(rd, "dump")
         env["ESDG_REF_INJECT"] = os.path.join(rd, "inject")
         env["ESDG_REF_KCACHE"] = os.path.join(HERE, "_ref", "kcache")
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
         p = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {EXE} {mode}"], cwd=rd, env=env,
                            capture_output=True, text=True, timeout=timeout)
+        if want_q and p.returncode == 0:
+            names = seq_names(params.PositivityPreserving, int(getattr(params, "PartialDryTreatment", 0)),
+                              int(getattr(params, "ArrivalTimings", 0)), int(getattr(params, "maximumElevation", 0)))
+            with open(os.path.join(rd, "dump", "manifest.txt")) as f:
+                mem = {int(w[1]): int(w[3]) for w in (ln.split() for ln in f) if w[0] == "from"}
+            q_final = np.fromfile(os.path.join(rd, "dump", f"to_{mem[names.index('q')]:03d}.bin"), dtype=np.float64)
     finally:
         shutil.rmtree(rd, ignore_errors=True)
     m = re.search(r"time taken in seconds = ([0-9.eE+-]+)", p.stdout)
     if p.returncode != 0 or not m:
         raise RuntimeError(f"reference run failed ({p.returncode}):\n{p.stdout[-2000:]}\n{p.stderr[-2000:]}")
-    return float(m.group(1)), p.stdout
+    return float(m.group(1)), p.stdout, q_final
 
 
 def warm_kernels(params, mesh_file, mode="OpenMP"):
