@@ -182,6 +182,27 @@ def case_conv_tc1(name="conv_tc1_N3"):
                              "state": "Testcase 1 manufactured solution"})
 
 
+def case_shipped_mesh(name, mesh, N, state, T):
+    """A run on one of the reference's own meshes (meshFiles/), read by its
+    reader: a circular dam break on a flat bottom, or a lake at rest over
+    Gaussian bumps with a ripple; plain path, walls."""
+    params = host.Params(N=N, CFL=0.4, T=T, NumFlux=0, rkOrder=4, rkSSP=0)
+    mf = f"meshFiles/{mesh}"
+    setup = run_ref.run(name + "_setup", params, mesh_file=mf)
+    x, y = setup["x"], setup["y"]
+    if state == "dam":
+        b = np.zeros_like(x)
+        cx, cy = 0.5 * (x.min() + x.max()), 0.5 * (y.min() + y.max())
+        r = 0.25 * (x.max() - x.min())
+        h = np.where((x - cx) ** 2 + (y - cy) ** 2 < r * r, 1.5, 1.0)
+    else:
+        b, h = gaussian_state(x, y, seed=13)
+    Bx, By = bottom_derivs(setup, N, b)
+    out = run_ref.run(name, params, mesh_file=mf, inject={"q": pack_q(h, n2=(N + 1) ** 2), "b": b, "Bx": Bx,
+                                                          "By": By})
+    save(name, params, out, {"mesh": f"reference meshFiles/{mesh}", "state": state})
+
+
 def case_analysis(name="walls_analysis_N3"):
     """Arrival times and maximum elevation (okl/Analysis/*): a ripple on a
     lake whose still-water level is 0 (b = -depth), walls.  The reference
@@ -220,6 +241,8 @@ CASES = {
     "island_pd_N3": lambda: case_island_pd(),
     "conv_tc1_N3": lambda: case_conv_tc1(),
     "walls_analysis_N3": lambda: case_analysis(),
+    "curvedam_N3": lambda: case_shipped_mesh("curvedam_N3", "CurveDamN3.mesh", 3, "dam", 0.05),
+    "pxy4_lake_N4": lambda: case_shipped_mesh("pxy4_lake_N4", "PeriodicXandY4.mesh", 4, "lake", 0.05),
 }
 
 

@@ -126,14 +126,19 @@ def test_bottom_derivatives_match_reference_algorithm():
 
 @pytest.mark.skipif(not __import__("oracle.run_ref", fromlist=["available"]).available(),
                     reason="reference tree not present")
-def test_reader_matches_reference_on_shipped_curved_mesh():
-    """Mesh::ReadMesh on the reference's own CircleInCircle.mesh (curved
-    boundaries of order 6, 83 reversed faces) vs the engine's reader."""
+@pytest.mark.parametrize("fixture,mesh_file,N", [("circle_lake_N3", "CircleInCircle.mesh", 3),
+                                                  ("curvedam_N3", "CurveDamN3.mesh", 3),
+                                                  ("pxy4_lake_N4", "PeriodicXandY4.mesh", 4)])
+def test_reader_matches_reference_on_shipped_curved_mesh(fixture, mesh_file, N):
+    """Mesh::ReadMesh on the reference's own meshes (CircleInCircle.mesh:
+    curved boundaries of order 6, 83 reversed faces; CurveDamN3.mesh: 1600
+    elements, order 3; PeriodicXandY4.mesh: 16 elements, order 4) vs the
+    engine's reader."""
     import os
     from oracle import run_ref
-    _, _, z = fixtures.load("circle_lake_N3")
-    mesh = host.mesh_read(3, os.path.join(run_ref.REF, "meshFiles", "CircleInCircle.mesh"))
-    _compare_setup(mesh, host.Basis.build(3), z)
+    _, _, z = fixtures.load(fixture)
+    mesh = host.mesh_read(N, os.path.join(run_ref.REF, "meshFiles", mesh_file))
+    _compare_setup(mesh, host.Basis.build(N), z)
 
 
 def test_okada_matches_reference_routine():
