@@ -1,9 +1,10 @@
 """The oracle against the reference program, live, on the problems the GPU
 parity tests compare the engine with the oracle on (CPU).
 
-tests/test_gpu_parity.py and test_gpu_av_pp.py hold the engine to the
-oracle on rotated curved meshes (every face-orientation pairing), NumFlux 3,
-SSP-RK3 and the artificial-viscosity path.  Here the reference program
+tests/test_gpu_parity.py, test_gpu_av_pp.py and test_gpu_partial_dry.py
+hold the engine to the oracle on rotated curved meshes (every
+face-orientation pairing), NumFlux 3, SSP-RK3, the artificial-viscosity
+path, and the partial-dry treatment with artificial viscosity.  Here the reference program
 (oracle/_ref/esdg_ref) runs the same problems -- the mesh written as ISM-V2
 by the engine's writer and read by the reference's reader, state and
 bathymetry injected -- and the oracle must end in its state bit for bit, so
@@ -29,6 +30,20 @@ def _ssp(pr):
     return pr
 
 
+def _island_av():
+    """The partial-dry island of tests/golden/island_pd_N3.npz with the
+    artificial viscosity on top (tests/test_gpu_partial_dry.py)."""
+    import dataclasses
+    from tests.golden import fixtures
+    prob = fixtures.load("island_pd_N3")[0]
+    p = dataclasses.replace(prob.params, ArtificialViscosity=1, epsilon_0=0.002, sigma_min=-6.0, sigma_max=-2.0,
+                            DFL=0.1)
+    fd = prob.basis.fd_mats
+    prob = host.make_problem(p, prob.mesh, prob.b, prob.q0, prob.meta)
+    prob.basis.fd_mats = fd
+    return prob
+
+
 CASES = {
     # (problem, mesh arguments as the problem builds its mesh, end time)
     "curved_rot_nf3_N3": (lambda: problems.curved_lake(N=3, nel=12, seed=3, ripple=0.02, NumFlux=3, rotate_seed=7),
@@ -41,6 +56,8 @@ CASES = {
     "dam_av_rot_N3": (lambda: problems.dam_break(N=3, nel=12, seed=2, rotate_seed=5), dict(N=3, nel=12, rot=5),
                       0.005),
     "dam_av_N4": (lambda: problems.dam_break(N=4, nel=12, seed=2), dict(N=4, nel=12, rot=0), 0.005),
+    # Cartesian mesh of the reference's own generator: (xL, xR, yL, yR, NX, NY, periodic rows, columns)
+    "island_pd_av_N3": (_island_av, dict(cart=(0.0, 1.0, 0.0, 1.0, 12, 12, 0, 0)), 0.004),
 }
 
 
@@ -48,15 +65,18 @@ CASES = {
 def test_oracle_matches_reference_program(name, tmp_path):
     make, m, T = CASES[name]
     pr = make()
-    path = str(tmp_path / f"{name}.mesh")
-    mesh = host.mesh_mapped(m["N"], 0.0, 1.0, 0.0, 1.0, m["nel"], m["nel"], amp=0.03, rotate_seed=m["rot"],
-                            write_path=path)
-    np.testing.assert_array_equal(mesh.x, pr.mesh.x)  # the problem's own mesh
+    if "cart" in m:
+        where = dict(cartesian=m["cart"])
+    else:
+        path = str(tmp_path / f"{name}.mesh")
+        mesh = host.mesh_mapped(m["N"], 0.0, 1.0, 0.0, 1.0, m["nel"], m["nel"], amp=0.03, rotate_seed=m["rot"],
+                                write_path=path)
+        np.testing.assert_array_equal(mesh.x, pr.mesh.x)  # the problem's own mesh
+        where = dict(mesh_file=path)
     p = pr.params
     p.T = T
     try:
-        out = run_ref.run(f"live_{name}", p, mesh_file=path,
-                          inject={"q": pr.q0, "b": pr.b, "Bx": pr.Bx, "By": pr.By})
+        out = run_ref.run(f"live_{name}", p, inject={"q": pr.q0, "b": pr.b, "Bx": pr.Bx, "By": pr.By}, **where)
     finally:
         shutil.rmtree(os.path.join(run_ref.HERE, "_ref", "runs", f"live_{name}"), ignore_errors=True)
     ref = OracleProblem(pr).run(T=T, max_steps=0)
