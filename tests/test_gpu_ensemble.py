@@ -61,3 +61,27 @@ def test_continuous_batching_refill_mid_flight():
         np.testing.assert_array_equal(ens.q(ic), alone(c, 9)[0])
     finally:
         ens.close()
+
+
+def test_tsunami_member_alone_matches_oracle():
+    """An ensemble member at its own scales (2000 km square, 4000 m shelf,
+    Okada uplift, artificial viscosity) run alone by the engine against the
+    oracle (which equals the reference program on it bit for bit,
+    tests/test_reference_live_cpu.py): relative L2 per variable <= 1e-12
+    (the shock sensor's log10 and sin differ in the last ulp between CUDA
+    and glibc)."""
+    from oracle.oracle import OracleProblem
+    pr = problems.tsunami_member(3, N=3, steps=0, sizes=(16,))
+    s = Solver(pr)
+    try:
+        t, n = s.run(T=300.0, max_steps=0)
+        q = s.q()
+    finally:
+        s.close()
+    ref = OracleProblem(pr).run(T=300.0, max_steps=0)
+    assert n == ref["steps"] >= 3 and t == pytest.approx(300.0, abs=1e-9)
+    K, n2 = pr.K, pr.ngl ** 2
+    a, b = q.reshape(K, 3, n2), ref["q"].reshape(K, 3, n2)
+    for v in range(3):
+        err = np.linalg.norm(a[:, v] - b[:, v]) / np.linalg.norm(b[:, v])
+        assert err <= 1e-12, (v, err)
