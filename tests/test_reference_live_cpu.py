@@ -58,6 +58,8 @@ CASES = {
     "dam_av_N4": (lambda: problems.dam_break(N=4, nel=12, seed=2), dict(N=4, nel=12, rot=0), 0.005),
     # Cartesian mesh of the reference's own generator: (xL, xR, yL, yR, NX, NY, periodic rows, columns)
     "island_pd_av_N3": (_island_av, dict(cart=(0.0, 1.0, 0.0, 1.0, 12, 12, 0, 0)), 0.004),
+    # the manufactured-solution test (Testcase 1) at N = 4 (tests/test_gpu_convergence.py)
+    "conv_tc1_N4": (lambda: problems.conv_test(N=4, nel=6), dict(cart=(0.0, 2.0, 0.0, 2.0, 6, 6, 0, 0)), 0.02),
     # an ensemble member at its own scales: 2000 km square, 4000 m shelf, Okada uplift, viscosity on
     "tsunami_av_N3": (lambda: problems.tsunami_member(3, N=3, steps=0, sizes=(16,)),
                       dict(cart=(0.0, 2.0e6, 0.0, 2.0e6, 16, 16, 0, 0)), 300.0),
