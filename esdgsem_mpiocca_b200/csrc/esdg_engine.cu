@@ -274,6 +274,8 @@ class Engine {
         if (ArrivalTimes_) {
             if ((r = alloc(&arrival, nn))) return r;
             k_fill_f64<<<(unsigned)((nn + 255) / 256), 256>>>(arrival, (long)nn, 1000.0);
+            const cudaError_t le = cudaGetLastError();
+            if (le != cudaSuccess) return cuda_fail(le, "arrival-time fill");
         }
         if (MaxElevation_ && (r = alloc(&max_elev, nn))) return r;  // from 0, as the reference's calloc
         if ((r = alloc(&st, (size_t)I))) return r;
