@@ -237,9 +237,11 @@ def reference_program_sample(prob, threads):
         path = os.path.join(d, "curved_lake.mesh")
         host.mesh_mapped(N_POLY, 0.0, 1.0, 0.0, 1.0, NEL, NEL, amp=0.03, write_path=path)
         inject = {"q": prob.q0, "b": prob.b, "Bx": prob.Bx, "By": prob.By}
-        w = run_ref.run_timed(reference_params(prob, REF_WARMUP_STEPS), path, inject, threads=threads)[0]
+        # about 10 s of set-up and 0.4-1 s per step on 8-16 cores; the bound keeps the leg within minutes
+        w = run_ref.run_timed(reference_params(prob, REF_WARMUP_STEPS), path, inject, threads=threads,
+                              timeout=240)[0]
         wk = run_ref.run_timed(reference_params(prob, REF_WARMUP_STEPS + REF_SAMPLE_STEPS), path, inject,
-                               threads=threads)[0]
+                               threads=threads, timeout=240)[0]
     finally:
         shutil.rmtree(d, ignore_errors=True)
     el = wk - w
