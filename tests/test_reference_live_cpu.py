@@ -58,6 +58,13 @@ CASES = {
     "dam_av_N4": (lambda: problems.dam_break(N=4, nel=12, seed=2), dict(N=4, nel=12, rot=0), 0.005),
     # Cartesian mesh of the reference's own generator: (xL, xR, yL, yR, NX, NY, periodic rows, columns)
     "island_pd_av_N3": (_island_av, dict(cart=(0.0, 1.0, 0.0, 1.0, 12, 12, 0, 0)), 0.004),
+    # higher degrees on a rotated curved mesh
+    "curved_rot_nf0_N5": (lambda: problems.curved_lake(N=5, nel=8, seed=5, ripple=0.05, rotate_seed=3),
+                          dict(N=5, nel=8, rot=3), 0.01),
+    "curved_rot_nf3_N6": (lambda: problems.curved_lake(N=6, nel=6, seed=6, ripple=0.05, NumFlux=3, rotate_seed=9),
+                          dict(N=6, nel=6, rot=9), 0.01),
+    "curved_rot_nf0_N7": (lambda: problems.curved_lake(N=7, nel=5, seed=7, ripple=0.05, rotate_seed=4),
+                          dict(N=7, nel=5, rot=4), 0.01),
     # the manufactured-solution test (Testcase 1) at N = 4 (tests/test_gpu_convergence.py)
     "conv_tc1_N4": (lambda: problems.conv_test(N=4, nel=6), dict(cart=(0.0, 2.0, 0.0, 2.0, 6, 6, 0, 0)), 0.02),
     # an ensemble member at its own scales: 2000 km square, 4000 m shelf, Okada uplift, viscosity on
