@@ -1618,13 +1618,14 @@ int esdg_diagnostics(int K, int N, const double* wGL, const double* Jinv, const 
 // ===========================================================================
 // Right-hand side without any allocation (esdg_compute_rhs_noalloc).
 //
-// For callers that may not allocate device memory themselves: code that runs
-// while a stream is being captured into a CUDA graph, hosts whose memory is
-// owned by their own pool allocator, and serving loops that must not stall
-// on cudaMalloc/cudaFree (both synchronise the device).  They pass their own
-// device buffers for the inputs and the output; the scratch this evaluation
-// needs (packed face/side tables, bathymetry traces, face fluxes, a step
-// state) lives in one file-scope device array of fixed size.
+// For callers that may not allocate device memory themselves: hosts whose
+// memory is owned by their own pool allocator, and serving loops that must
+// not stall on cudaMalloc/cudaFree (both synchronise the device).  They pass
+// their own device buffers for the inputs and the output; the scratch this
+// evaluation needs (packed face/side tables, bathymetry traces, face fluxes,
+// a step state) lives in one file-scope device array of fixed size.  The
+// call reads the count of bad connectivity entries back to the host and
+// synchronises its stream before it returns.
 // ===========================================================================
 namespace esdg {
 
@@ -1743,7 +1744,7 @@ extern "C" int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES
     if (L.total > kNoAllocScratchDoubles) {
         g_create_error = "compute_rhs_noalloc: mesh needs " + std::to_string(L.total) +
                          " doubles of scratch, the fixed maximum is " + std::to_string(kNoAllocScratchDoubles) +
-                         " (about 5*Nfaces*(N+1) + 8*Nelem)";
+                         " (2*Nfaces + 8*Nelem + 5*Nfaces*(N+1), tables rounded up to 256 bytes)";
         return ESDG_E_ARG;
     }
     int dev = 0;
@@ -1751,6 +1752,20 @@ extern "C" int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES
     if (e != cudaSuccess || dev < 0 || dev >= 64) {
         g_create_error = std::string("compute_rhs_noalloc: cudaGetDevice: ") + cudaGetErrorString(e);
         return ESDG_E_CUDA;
+    }
+    if (stream) {
+        // the kernels run on `stream` against this device's scratch address
+        int sdev = -1;
+        e = cudaStreamGetDevice(static_cast<cudaStream_t>(stream), &sdev);
+        if (e != cudaSuccess) {
+            g_create_error = std::string("compute_rhs_noalloc: cudaStreamGetDevice: ") + cudaGetErrorString(e);
+            return ESDG_E_ARG;
+        }
+        if (sdev != dev) {
+            g_create_error = "compute_rhs_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                             ", the current device is " + std::to_string(dev) + "; make the stream's device current";
+            return ESDG_E_ARG;
+        }
     }
     double* base = nullptr;
     {

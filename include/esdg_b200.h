@@ -149,23 +149,26 @@ int esdg_copy_maximum_elevation(esdg_deviceclass* d, double* maximum_elevation);
 long long esdg_kernel_launches(const esdg_deviceclass* d);
 
 /* Same evaluation as esdg_compute_rhs, for callers that must not allocate
- * device memory (no counterpart in the reference): code running while a
- * stream is captured into a CUDA graph, hosts whose device memory belongs to
- * their own pool allocator, serving loops that cannot afford the device-wide
- * synchronisation of cudaMalloc/cudaFree.  Every pointer is a device pointer
- * the caller owns, in the layouts of esdg_copy_device_variables (Jinv = 1/J,
- * Dmat the flux-differencing matrix); Qt [K*3*(N+1)^2] receives L(q).  The
- * scratch (packed tables, bathymetry traces, face fluxes, one step state)
- * is a fixed 16 MiB device array inside this library, held by every GPU
- * that loads it until the process exits; a mesh needing more than that
- * (about 5*F*(N+1) + 8*K doubles) is rejected with ESDG_E_ARG.  The first
- * call on a device looks the array's address up (cudaGetSymbolAddress) with
- * that device current: make that first call before any stream capture.
- * All calls share the one array, so calls that overlap on the GPU race;
- * every call rewrites the parts it reads.  Out-of-range connectivity is
- * replaced by safe entries and reported as ESDG_E_ARG.  Runs on `stream`
- * (NULL: legacy default stream) and returns after it has finished; the
- * message of a failure is esdg_last_error(NULL). */
+ * device memory (no counterpart in the reference): hosts whose device memory
+ * belongs to their own pool allocator, and serving loops that cannot afford
+ * the device-wide synchronisation of cudaMalloc/cudaFree.  Every pointer is a
+ * device pointer the caller owns, in the layouts of esdg_copy_device_variables
+ * (Jinv = 1/J, Dmat the flux-differencing matrix); Qt [K*3*(N+1)^2] receives
+ * L(q).  The scratch (packed tables, bathymetry traces, face fluxes, one step
+ * state) is a fixed 16 MiB device array inside this library (2^21 doubles),
+ * held by every GPU that loads it until the process exits.  A mesh needs
+ * 2*F + 8*K + 5*F*(N+1) doubles of it plus the step state and an error
+ * count, each table rounded up to 256 bytes; a mesh needing more than the
+ * array is rejected with ESDG_E_ARG.  The first call on a device looks the
+ * array's address up (cudaGetSymbolAddress) with that device current: make
+ * that first call before any stream capture.  A stream given must belong to
+ * the current device (ESDG_E_ARG otherwise).  All calls share the one array,
+ * so calls that overlap on the GPU race; every call rewrites the parts it
+ * reads.  Out-of-range connectivity is replaced by safe entries and reported
+ * as ESDG_E_ARG.  Runs on `stream` (NULL: legacy default stream); the call
+ * copies the count of bad connectivity entries back to the host and
+ * synchronises `stream` before it returns.  The message of a failure is
+ * esdg_last_error(NULL). */
 int esdg_compute_rhs_noalloc(int N, int K, int F, int NumFlux, int ES, double g_const, double PosPresTOL,
                              const double* q, const double* Jinv, const double* y_xi, const double* y_eta,
                              const double* x_xi, const double* x_eta, const double* Bx, const double* By,

@@ -2,21 +2,25 @@
 # ORACLE test infrastructure: compiles the reference program (main.cpp and
 # src/*.cpp of ESDGSEM_MPIOCCA, read where they lie, unmodified) against the
 # OCCA-v0 shim and the single-rank MPI stub in oracle/ref_shim/.  Output only
-# under oracle/_ref/.  The reference tree defaults to /root/reference.
+# under oracle/_ref/.  The reference tree is $ESDG_REFERENCE, else a checkout
+# named `reference` beside this repository.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${ESDG_REFERENCE:-/root/reference}
+REF=${ESDG_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}
 OUT="$HERE/_ref"
 mkdir -p "$OUT/obj"
 FLAGS="-O2 -ffp-contract=off -w -std=gnu++14 -I$HERE/ref_shim -I$REF/include"
-for f in "$REF"/src/*.cpp "$REF"/main.cpp "$HERE"/ref_shim/occa_shim.cpp; do
+for f in "$REF"/src/*.cpp "$REF"/main.cpp "$HERE"/ref_shim/occa_shim.cpp "$HERE"/ref_shim/bench_case.cpp; do
   o="$OUT/obj/$(basename "$f" .cpp).o"
-  if [ ! -f "$o" ] || [ "$f" -nt "$o" ]; then
+  if [ ! -f "$o" ] || [ "$f" -nt "$o" ] || [ "$HERE/ref_shim/occa.hpp" -nt "$o" ] || [ "$HERE/ref_shim/mpi.h" -nt "$o" ]; then
     g++ $FLAGS -Ddfloat=double -Ddfloat4=double4 -DMPI_DFLOAT=MPI_DOUBLE '-DdfloatString="double"' \
         '-Ddfloat4String="double4"' -c "$f" -o "$o"
   fi
 done
-g++ -o "$OUT/esdg_ref" "$OUT"/obj/*.o -ldl
+# SW2D::InitB / SW2D::InitQ calls from main.cpp go through the case hook
+# (oracle/ref_shim/bench_case.cpp), which forwards them unless ESDG_REF_CASE is set
+WRAP="-Wl,--wrap=_ZN4SW2D5InitBEi16MeshPartitioningiiiPKdS2_Pd -Wl,--wrap=_ZN4SW2D5InitQEi16MeshPartitioningiiiPKdS2_PddS2_dd"
+g++ -o "$OUT/esdg_ref" "$OUT"/obj/*.o -ldl $WRAP
 echo "$OUT/esdg_ref"
 # the reference's Okada routine alone, on points from a file
 g++ $FLAGS -Ddfloat=double -Ddfloat4=double4 -DMPI_DFLOAT=MPI_DOUBLE '-DdfloatString="double"' \

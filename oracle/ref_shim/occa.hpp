@@ -15,7 +15,10 @@
 //   ESDG_REF_INJECT=<dir> a copyFrom(host) with sequence number NNN takes its
 //                         bytes from <dir>/from_NNN.bin when that file exists
 //                         (same size required), i.e. a chosen initial state
-//                         and bathymetry replace the testcase's.
+//                         and bathymetry replace the testcase's;
+//   ESDG_REF_COUNT=1      at exit, the number of calls of every kernel is
+//                         printed ("[occa shim] calls <kernel> <n>"), which
+//                         gives the number of time steps a run took.
 #pragma once
 
 #include <cstddef>
@@ -84,12 +87,15 @@ struct arg<memory, void> {
 };
 }  // namespace detail
 
+void note_kernel_call(const std::string& name);
+
 class kernel {
   public:
     void* fn = nullptr;
     std::string name;
     template <class... A>
     void operator()(const A&... a) const {
+        note_kernel_call(name);
         typedef void (*F)(typename detail::arg<A>::type...);
         reinterpret_cast<F>(fn)(detail::arg<A>::conv(a)...);
     }

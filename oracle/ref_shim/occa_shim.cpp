@@ -34,6 +34,24 @@ static void manifest(const std::string& line) {
     f << line << "\n";
 }
 
+static std::map<std::string, long>& call_counts() {
+    static std::map<std::string, long> m;
+    return m;
+}
+
+static void print_call_counts() {
+    for (auto& kv : call_counts()) std::printf("[occa shim] calls %s %ld\n", kv.first.c_str(), kv.second);
+    std::fflush(stdout);
+}
+
+void note_kernel_call(const std::string& name) {
+    static const bool on = env("ESDG_REF_COUNT") != nullptr;
+    if (!on) return;
+    auto& m = call_counts();
+    if (m.empty()) std::atexit(print_call_counts);
+    ++m[name];
+}
+
 void printAvailableDevices() { std::cout << "[occa shim] Serial / OpenMP host modes\n"; }
 
 void kernelInfo::addDefine(const std::string& n, double v) {

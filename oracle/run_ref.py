@@ -25,7 +25,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("ESDG_REFERENCE", "/root/reference")
+# The reference source tree: $ESDG_REFERENCE, else a checkout named
+# `reference` beside this repository.
+REF = os.environ.get("ESDG_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 EXE = os.path.join(HERE, "_ref", "esdg_ref")
 
 # copyDeviceVariables argument order (src/deviceclass.cpp:576-626) as seen by
@@ -160,9 +162,11 @@ def _prepare(rd, params, mesh_file, inject, cartesian=None):
             os.symlink(os.path.join(REF, d), os.path.join(rd, d))
 
 
-def run_timed(params, mesh_file, inject=None, threads=None, mode="OpenMP", timeout=900, want_q=False):
+def run_timed(params, mesh_file, inject=None, threads=None, mode="OpenMP", timeout=900, want_q=False,
+              extra_env=None):
     """One run of the reference program on an absolute mesh path, state and
-    bathymetry injected as in `run`.  Returns (seconds, stdout, q_final):
+    bathymetry injected as in `run` (extra_env: further environment, e.g.
+    ESDG_REF_CASE for the case hook of oracle/ref_shim/bench_case.cpp).  Returns (seconds, stdout, q_final):
     the time its own timer reports around DGtimeloop (main.cpp:1009-1072,
     printed as "time taken in seconds"), and with want_q the final state
     (o_q.copyTo at main.cpp:1051, through the dump hook; None otherwise)."""
@@ -183,6 +187,7 @@ def run_timed(params, mesh_file, inject=None, threads=None, mode="OpenMP", timeo
         env["ESDG_REF_KCACHE"] = os.path.join(HERE, "_ref", "kcache")
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
+        env.update(extra_env or {})
         p = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {EXE} {mode}"], cwd=rd, env=env,
                            capture_output=True, text=True, timeout=timeout)
         if want_q and p.returncode == 0:
@@ -210,3 +215,9 @@ def warm_kernels(params, mesh_file, mode="OpenMP"):
         build()
     run_timed(params, mesh_file, None, threads=2, mode=mode, timeout=600)
     return True
+
+
+def kernel_calls(stdout):
+    """Kernel call counts the OCCA stand-in prints at exit with ESDG_REF_COUNT=1."""
+    import re
+    return {m.group(1): int(m.group(2)) for m in re.finditer(r"\[occa shim\] calls (\S+) (\d+)", stdout)}
