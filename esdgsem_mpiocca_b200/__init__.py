@@ -46,6 +46,9 @@ def _declare(lib):
         "esdg_set_stream": (_I, [_VP, _VP]),
         "esdg_advance": (_I, [_VP, _I, _D, _PD, _PI]),
         "esdg_profile_steps": (_I, [_VP, _I, _PD, _PD]),
+        "esdg_debug_bulk_wait_test": (_I, [_VP, ctypes.c_longlong, _I]),
+        "esdg_set_pause": (_I, [_VP, _D]),
+        "esdg_resume": (_I, [_VP, _PD, _PI]),
         "esdg_compute_rhs_noalloc": (_I, [_I, _I, _I, _I, _I, _D, _D] + [_VP] * 17 + [_VP, _VP]),
         "esdg_basis": (_I, [_I, _I] + [_PD] * 9),
         "esdg_basis_fd": (_I, [_I, _PD, _PD, _PD]),

@@ -468,7 +468,24 @@ class Engine {
             a.dry = dry; a.Bn = B; a.Dc = DcFD; a.Dup = DupFD; a.Ddn = DdnFD;
         }
         if (conv) { a.conv = 1; a.tfrac = stage_tfrac; a.X = X; a.Y = Y; }
+        a.wait_limit = dbg_wait_limit;
+        a.skip_tile = dbg_skip_tile;
         return a;
+    }
+
+    // Test hook of the bounded bulk-copy waits (esdg_debug_bulk_wait_test):
+    // the wait limit in clock cycles (0: the default) and a tile whose copies
+    // are never issued (tile + 1; 0: none).
+    long long dbg_wait_limit = 0;
+    int dbg_skip_tile = 0;
+
+    int set_bulk_wait_test(long long limit, int skip_tile) {
+        if (!built) return fail(ESDG_E_ARG, "bulk-wait test hook before buildDeviceKernels");
+        if (limit < 0 || skip_tile < -1) return fail(ESDG_E_ARG, "bulk-wait test hook: limit >= 0, tile >= -1");
+        dbg_wait_limit = limit;
+        dbg_skip_tile = skip_tile + 1;
+        if (graph) return capture_step_graph();
+        return 0;
     }
 
     // Plain-path element kernel: a persistent bulk-copy-pipelined kernel when
@@ -1018,6 +1035,7 @@ class Engine {
         std::memset(&s0, 0, sizeof(s0));
         s0.t = 0.0; s0.T = T; s0.minEle = minEle; s0.CFL = CFL; s0.DFL = DFL;
         s0.max_steps = max_steps;
+        s0.pause_on = pause_on; s0.pause_at = pause_at; s0.resume_steps = 0;
         *st_host = s0;
         cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) return cuda_fail(e, "state upload");
@@ -1027,6 +1045,45 @@ class Engine {
         if ((r = capture_step_graph())) return r;
         if ((r = run_steps(max_steps > 0 ? max_steps : 0))) return r;
         if ((r = poll_state())) return r;
+        if (t_out) *t_out = st_host->t;
+        if (steps_out) *steps_out = st_host->steps;
+        if (st_host->status == ST_NONFINITE)
+            return fail(ESDG_E_NONFINITE, "non-finite wave speed: the solution blew up (step " +
+                                              std::to_string(st_host->steps) + ")");
+        if (st_host->status == ST_TIMEOUT) return fail(ESDG_E_CUDA, "a bulk copy did not complete (bounded wait)");
+        return 0;
+    }
+
+    // Checkpoint pause of the time loop (esdg_set_pause / esdg_resume).
+    int pause_on = 0;
+    double pause_at = 0.0;
+
+    int set_pause(double t_pause) {
+        pause_on = std::isfinite(t_pause) ? 1 : 0;
+        pause_at = pause_on ? t_pause : 0.0;
+        return 0;
+    }
+
+    // Continues a loop that stopped at a pause: at least one step, then
+    // until the next pause, T or the step cap of esdg_dg_timeloop.
+    int resume(double* t_out, int* steps_out) {
+        int r = check_ready();
+        if (r) return r;
+        if (!graph) return fail(ESDG_E_ARG, "esdg_resume needs a previous esdg_dg_timeloop call");
+        if ((r = poll_state())) return r;
+        const bool finished = !(st_host->t < st_host->T) ||
+                              (st_host->max_steps > 0 && st_host->steps >= st_host->max_steps) ||
+                              st_host->status != ST_OK;
+        if (!finished) {
+            st_host->done = 0;
+            st_host->pause_on = pause_on;
+            st_host->pause_at = pause_at;
+            st_host->resume_steps = st_host->steps;
+            cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "state upload");
+            if ((r = run_steps(0))) return r;
+            if ((r = poll_state())) return r;
+        }
         if (t_out) *t_out = st_host->t;
         if (steps_out) *steps_out = st_host->steps;
         if (st_host->status == ST_NONFINITE)
@@ -1060,6 +1117,7 @@ class Engine {
         if (t_out) *t_out = st_host->t;
         if (steps_out) *steps_out = st_host->steps;
         if (st_host->status == ST_NONFINITE) return fail(ESDG_E_NONFINITE, "non-finite wave speed");
+        if (st_host->status == ST_TIMEOUT) return fail(ESDG_E_CUDA, "a bulk copy did not complete (bounded wait)");
         return 0;
     }
 
@@ -1241,7 +1299,7 @@ int esdg_init_device_variables(esdg_deviceclass* d, int N, int Nelem, int Nfaces
                                int CreateTimeSeries, int CalcMaximumElevation) {
     ESDG_GUARD(d);
     (void)NEpad; (void)NEsurfpad; (void)Nedgepad; (void)NAvgPad;  // launch shapes are chosen per ngl
-    (void)CreateTimeSeries;  // gauge time series are written by the reference's plot checkpoints: not rebuilt
+    (void)CreateTimeSeries;  // gauge series: written by the C++ facade at the plot checkpoints
     return d->eng.init(N, Nelem, Nfaces, rank, rkSSP, ES, Testcase, epsilon_0, sigma_max, sigma_min, PosPresTOL,
                        geomface, g_const, PositivityPreserving, ArtificialViscosity, DiscBottom, h_0, PartialDry,
                        FrictionTerms, CalcArrivalTimes, CalcMaximumElevation);
@@ -1283,6 +1341,7 @@ int esdg_dg_timeloop(esdg_deviceclass* d, int Nelem, int Nfaces, int rkStages, c
                      int PlotVar, int EntropyPlot, int PositivityPreserving, int DiscBottom, int max_steps,
                      double* t_out, int* steps_out) {
     ESDG_GUARD(d);
+    // plot outputs are the C++ facade's (checkpoints through esdg_set_pause / esdg_resume)
     (void)NumPlots; (void)NumTimeChecks; (void)PlotVar; (void)EntropyPlot; (void)Testcase;
     esdg::Engine& E = d->eng;
     if (Nelem != E.K || Nfaces != E.F) return E.fail(ESDG_E_ARG, "Nelem/Nfaces differ from initDeviceVariables");
@@ -1441,6 +1500,21 @@ int esdg_profile_steps(esdg_deviceclass* d, int nsteps, double* face_ms, double*
     ESDG_GUARD(d);
     if (nsteps <= 0 || !face_ms || !elem_ms) return d->eng.fail(ESDG_E_ARG, "bad profile_steps arguments");
     return d->eng.profile_steps(nsteps, face_ms, elem_ms);
+}
+
+int esdg_set_pause(esdg_deviceclass* d, double t_pause) {
+    if (!d) return ESDG_E_ARG;
+    return d->eng.set_pause(t_pause);
+}
+
+int esdg_resume(esdg_deviceclass* d, double* t_out, int* steps_out) {
+    if (!d) return ESDG_E_ARG;
+    return d->eng.resume(t_out, steps_out);
+}
+
+int esdg_debug_bulk_wait_test(esdg_deviceclass* d, long long wait_limit_cycles, int skip_tile) {
+    if (!d) return ESDG_E_ARG;
+    return d->eng.set_bulk_wait_test(wait_limit_cycles, skip_tile);
 }
 
 int esdg_advance(esdg_deviceclass* d, int nsteps, double T, double* t_out, int* steps_out) {

@@ -31,6 +31,12 @@ struct DevState {
     double t, dt, T, minEle, CFL, DFL;
     unsigned long long lam_key, visc_key;
     int steps, max_steps, done, status;
+    // checkpoint pause (pause_on != 0): a step does not start once t >=
+    // pause_at and at least one step ran since steps == resume_steps; the
+    // host writes its outputs and resumes (the reference's plot checkpoints,
+    // src/deviceclass.cpp:1143-1147, one per step)
+    double pause_at;
+    int pause_on, resume_steps;
 };
 
 struct FaceArgs {
@@ -115,6 +121,12 @@ struct ElemArgs {
     double tfrac = 0.0;
     const double* __restrict__ X = nullptr;
     const double* __restrict__ Y = nullptr;
+    // Bounded waits of the bulk-copy kernels: limit in clock cycles (0: the
+    // default, about 2 s) and, for a test of the timeout path, a tile whose
+    // copies are never issued (tile + 1; 0: none).  Zero-initialised
+    // arguments leave both off.
+    long long wait_limit = 0;
+    int skip_tile = 0;
 };
 
 // r += the manufactured source of node xid (Testcase 1).
@@ -896,6 +908,7 @@ __global__ void k_step_begin(int I, DevState* st, int ngl, int AV) {
     DevState& s = st[k];
     if (s.done) return;
     if (!(s.t < s.T) || (s.max_steps > 0 && s.steps >= s.max_steps)) { s.done = 1; return; }
+    if (s.pause_on && s.steps > s.resume_steps && s.t >= s.pause_at) { s.done = 1; return; }
     const double lam = __longlong_as_double((long long)s.lam_key);
     if (s.lam_key == ~0ull || !isfinite(lam)) { s.status = ST_NONFINITE; s.done = 1; return; }
     const double dt_i = s.minEle / (double)ngl * s.CFL / lam;

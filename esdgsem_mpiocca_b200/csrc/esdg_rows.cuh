@@ -84,6 +84,7 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 template <int NGL, int NE, int ST>
 __device__ __forceinline__ void rows_issue_tile(const ElemArgs& a, int t, double* sb, uint64_t* bar) {
     using S = RowShape<NGL, NE, ST>;
+    if (t + 1 == a.skip_tile) return;  // test hook: this tile's copies are never issued
     const int e0 = t * NE;
     const int ne = min(NE, a.K - e0);
     const unsigned qb = (unsigned)(ne * 3 * S::N2 * sizeof(double));
@@ -210,10 +211,11 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
         const double dt = (active && a.mode != 2) ? a.st[ins].dt : 0.0;
         // a copy that never lands makes the whole CTA leave together
         // (uniform decision) with an error status for the host
-        const bool landed = mbar_wait_bounded(&bar[sidx], parity);
+        const bool landed = mbar_wait_bounded(&bar[sidx], parity, a.wait_limit);
         if (__syncthreads_or(!landed)) {
             if (tid == 0) {
                 atomicExch(&a.st[0].status, ST_TIMEOUT);
+                drain_stages<ST>(bar, it, t, ntiles, a.skip_tile, a.wait_limit);
                 bulk_wait_all();
             }
             return;

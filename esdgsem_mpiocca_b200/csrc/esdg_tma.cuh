@@ -54,14 +54,29 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Waits for the phase with the given parity; gives up after ~2 s of clock
-// (a copy that never lands), returning false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// Waits for the phase with the given parity; gives up after `limit` clock
+// cycles (0: 4e9, about 2 s; a copy that never lands), returning false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, long long limit = 0) {
     if (mbar_try_wait(bar, parity)) return true;
+    const long long lim = limit > 0 ? limit : 4000000000ll;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > 4000000000ll) return false;
+        if (clock64() - t0 > lim) return false;
     return true;
+}
+
+// After a wait ran out: the bulk copies of the stages still in flight
+// (iterations it+1 .. it+ST-1 of this CTA) land before the CTA returns and
+// its shared memory is released; bounded like every wait.  One thread.
+template <int ST>
+__device__ __forceinline__ void drain_stages(uint64_t* bar, int it, int t, int ntiles, int skip_tile,
+                                             long long limit) {
+#pragma unroll
+    for (int k = 1; k < ST; ++k) {
+        const int itk = it + k;
+        const int tk = t + k * (int)gridDim.x;
+        if (tk < ntiles && tk + 1 != skip_tile) mbar_wait_bounded(&bar[itk % ST], (unsigned)((itk / ST) & 1), limit);
+    }
 }
 
 // Entropy-conservative two-point flux of okl/DG/VolumeKernelFluxDiffV99.okl:17-57,
@@ -128,6 +143,7 @@ struct TmaShape {
 template <int NGL>
 __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double* sb, uint64_t* bar) {
     using S = TmaShape<NGL>;
+    if (t + 1 == a.skip_tile) return;  // test hook: this tile's copies are never issued
     const int e0 = t * S::NE;
     const int ne = min(S::NE, a.K - e0);
     const unsigned qb = (unsigned)(ne * 3 * S::N2 * sizeof(double));
@@ -222,9 +238,12 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
         // every thread waits for the tile; a copy that never lands makes the
         // whole CTA leave together (uniform decision) with an error status
         // for the host instead of hanging
-        const bool landed = mbar_wait_bounded(&bar[sidx], parity);
+        const bool landed = mbar_wait_bounded(&bar[sidx], parity, a.wait_limit);
         if (__syncthreads_or(!landed)) {
-            if (tid == 0) atomicExch(&a.st[0].status, ST_TIMEOUT);
+            if (tid == 0) {
+                atomicExch(&a.st[0].status, ST_TIMEOUT);
+                drain_stages<ST>(bar, it, t, ntiles, a.skip_tile, a.wait_limit);
+            }
             return;
         }
         const int s = el * N2 + nd;          // node slot in nodal sections

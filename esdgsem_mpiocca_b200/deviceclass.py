@@ -162,6 +162,12 @@ class DeviceClass:
     def kernel_launches(self) -> int:
         return int(self._L.esdg_kernel_launches(self.h))
 
+    def debug_bulk_wait_test(self, wait_limit_cycles: int, skip_tile: int):
+        """Test hook of the element kernels' bounded bulk-copy waits: a
+        shorter wait limit (clock cycles, 0: the default) and a tile whose
+        copies are never issued (-1: none)."""
+        self._ok(self._L.esdg_debug_bulk_wait_test(self.h, int(wait_limit_cycles), int(skip_tile)))
+
     def set_indicator(self, mode: int, net=None):
         """Indicator of the artificial-viscosity path: 0 the modal sensor and
         the viscous terms everywhere (the reference's path), 1 the modal

@@ -83,8 +83,12 @@ int esdg_build_device_kernels(esdg_deviceclass* d, int KernelVersion, int Kernel
  * src/deviceclass.cpp:630-1335.  The RungeKutta object is passed as its
  * tables (rkStages, CoeffsA/B/C); globalMinEleSize as computed by
  * basis::calcElementSizes.  max_steps > 0 additionally caps the number of
- * steps (the reference loop is time-driven only).  Plot/time-series
- * arguments are accepted and ignored (no Tecplot output).  On return
+ * steps (the reference loop is time-driven only).  The plot and
+ * time-series arguments (NumPlots, NumTimeChecks, PlotVar, EntropyPlot) are
+ * accepted and not used here: the C ABI writes no files.  The reference's
+ * outputs at its plot checkpoints are written by the C++ facade
+ * (include/esdg_deviceclass.hpp) around esdg_set_pause / esdg_resume below.
+ * The loop stops early at a pause set with esdg_set_pause.  On return
  * *t_out / *steps_out hold the reached time and the step count. */
 int esdg_dg_timeloop(esdg_deviceclass* d, int Nelem, int Nfaces, int rkStages, const double* rkA, const double* rkB,
                      const double* rkC, double globalMinEleSize, double CFL, double DFL, double T, int Testcase,
@@ -121,6 +125,30 @@ int esdg_compute_rhs(esdg_deviceclass* d, double* Qt_host, double* visc_host);
  * Lets a caller order the engine's kernels with its own work and time them
  * with its own events. */
 int esdg_set_stream(esdg_deviceclass* d, void* cuda_stream);
+
+/* Checkpoints of the time loop (src/deviceclass.cpp:797-838, 1143-1147: the
+ * reference writes its plots, entropy/mass and gauge series when, after a
+ * step, t >= the next checkpoint; one checkpoint per step).
+ * esdg_set_pause(d, t_pause): the following esdg_dg_timeloop / esdg_resume
+ * stops before a step starts once t >= t_pause, provided a step ran since
+ * the call began (non-finite t_pause: no pause).  Stepping is unchanged:
+ * dt is clipped only at T, as in the reference.  esdg_resume(d, t, steps)
+ * continues a paused loop (at least one step) until the next pause, T or the
+ * step cap; on a finished loop it returns at once.  Both return
+ * ESDG_E_NONFINITE / ESDG_E_CUDA as esdg_dg_timeloop does.  (No counterpart
+ * call in the reference: its DGtimeloop stops at checkpoints internally.) */
+int esdg_set_pause(esdg_deviceclass* d, double t_pause);
+int esdg_resume(esdg_deviceclass* d, double* t_out, int* steps_out);
+
+/* Test hook of the bounded bulk-copy waits (no counterpart in the
+ * reference; for tests only).  The persistent element kernels wait on each
+ * tile's bulk copies with a clock-cycle limit; a copy that never lands makes
+ * the CTA record a time-out, let its other copies in flight land (bounded as
+ * well) and return, and the run returns ESDG_E_CUDA.  wait_limit_cycles sets
+ * that limit (0: the default, about 2 s); skip_tile >= 0 names a tile whose
+ * copies are never issued, so that its wait runs out (-1: none).  Takes
+ * effect for the following launches (the step graph is captured again). */
+int esdg_debug_bulk_wait_test(esdg_deviceclass* d, long long wait_limit_cycles, int skip_tile);
 
 /* Advance the resident state by up to nsteps steps (same step as
  * esdg_dg_timeloop) without any host copy of q; the device-side time and

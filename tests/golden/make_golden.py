@@ -308,6 +308,48 @@ for _n in DROPIN_CASES:
     CASES[_n] = (lambda n: (lambda: make_dropin(n)))(_n)
 
 
+# The time loop's outputs (src/deviceclass.cpp:797-838, 1143-1309 and
+# src/Plots.cpp): plot checkpoints with the solution (PlotVar 1), total
+# entropy and mass over time (EntropyPlot), written by the reference program
+# into movie/; the drop-in driver must write the same files.
+DROPIN_OUTPUT_CASES = {
+    "dropin_outputs_tc20": dict(N=2, T=0.03, NumFlux=0, Testcase=20, cart=(-5.0, 5.0, -5.0, 5.0, 6, 6, 0, 0),
+                                NumPlots=4, EntropyPlot=1, PlotVar=1),
+}
+
+
+def make_dropin_outputs(name):
+    import shutil
+    import subprocess
+    spec = DROPIN_OUTPUT_CASES[name]
+    p = dropin_params(spec)
+    rd = os.path.join(ROOT, "oracle", "_ref", "runs", name)
+    if os.path.isdir(rd):
+        shutil.rmtree(rd)
+    os.makedirs(os.path.join(rd, "movie"))
+    for d in ("okl", "meshFiles", "data"):
+        os.symlink(os.path.join(run_ref.REF, d), os.path.join(rd, d))
+    run_ref.write_input(os.path.join(rd, "input.dat"), p, "none", 1)
+    run_ref.write_cartesian(os.path.join(rd, "Cartesian.dat"), *spec["cart"])
+    txt = open(os.path.join(rd, "input.dat")).read()
+    for k in ("NumPlots", "EntropyPlot", "PlotVar"):
+        txt = txt.replace(f"{k}={'2' if k == 'PlotVar' else '0'}\n", f"{k}={spec[k]}\n")
+    open(os.path.join(rd, "input.dat"), "w").write(txt)
+    env = dict(os.environ, ESDG_REF_KCACHE=os.path.join(ROOT, "oracle", "_ref", "kcache"))
+    out = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {run_ref.EXE} Serial"], cwd=rd, env=env,
+                         capture_output=True, text=True, timeout=600, check=True)
+    files = {f: open(os.path.join(rd, "movie", f)).read() for f in sorted(os.listdir(os.path.join(rd, "movie")))}
+    rec = {"spec": spec, "input_dat": txt, "cartesian_dat": open(os.path.join(rd, "Cartesian.dat")).read(),
+           "diagnostics": diag_lines(out.stdout), "movie": files}
+    with open(os.path.join(OUT, f"{name}.json"), "w") as f:
+        json.dump(rec, f, indent=1)
+    print(name, sorted(files))
+
+
+for _n in DROPIN_OUTPUT_CASES:
+    CASES[_n] = (lambda n: (lambda: make_dropin_outputs(n)))(_n)
+
+
 # ---------------------------------------------------------------------------
 # The reference's Okada routine (src/okada.cpp) on a lon/lat grid around the
 # epicentre of its shipped fault file data/indianOceanFault1.txt.

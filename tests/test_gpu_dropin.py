@@ -55,3 +55,29 @@ def test_reference_driver_on_engine_prints_reference_results(case, tmp_path):
             rk, rv = r.rsplit(" ", 1)
             assert gk == rk
             assert abs(float(gv) - float(rv)) <= rtol * abs(float(rv)) + atol, (g, r)
+
+
+OUTPUT_CASES = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "dropin_outputs_*.json")))
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="drop-in driver not built (oracle/build_ref.sh dropin)")
+@pytest.mark.parametrize("case", OUTPUT_CASES, ids=[os.path.basename(c)[:-5] for c in OUTPUT_CASES])
+def test_reference_driver_on_engine_writes_reference_outputs(case, tmp_path):
+    """Plot checkpoints (NumPlots), the solution plots (PlotVar 1) and the
+    entropy and mass series (EntropyPlot) that the reference program wrote
+    into movie/ (tests/golden/dropin_outputs_*.json): the drop-in driver on
+    the engine writes the same files, byte for byte -- including the
+    reference's one-checkpoint-per-step rule, which leaves a checkpoint
+    unwritten when one step crosses two."""
+    rec = json.load(open(case))
+    (tmp_path / "input.dat").write_text(rec["input_dat"])
+    (tmp_path / "Cartesian.dat").write_text(rec["cartesian_dat"])
+    (tmp_path / "movie").mkdir()
+    p = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {EXE} CUDA"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    got = {f: (tmp_path / "movie" / f).read_text() for f in sorted(os.listdir(tmp_path / "movie"))}
+    assert sorted(got) == sorted(rec["movie"])
+    for name, text in rec["movie"].items():
+        assert got[name] == text, name
+    assert diag_lines(p.stdout) == rec["diagnostics"]

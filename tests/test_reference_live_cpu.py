@@ -65,6 +65,11 @@ CASES = {
                           dict(N=6, nel=6, rot=9), 0.01),
     "curved_rot_nf0_N7": (lambda: problems.curved_lake(N=7, nel=5, seed=7, ripple=0.05, rotate_seed=4),
                           dict(N=7, nel=5, rot=4), 0.01),
+    # the lowest degrees: N = 1 (2x2 nodes) and N = 2 (tests/test_gpu_degrees.py)
+    "curved_rot_nf0_N1": (lambda: problems.curved_lake(N=1, nel=12, seed=8, ripple=0.05, rotate_seed=6),
+                          dict(N=1, nel=12, rot=6), 0.01),
+    "curved_rot_nf3_N2": (lambda: problems.curved_lake(N=2, nel=10, seed=9, ripple=0.05, NumFlux=3, rotate_seed=2),
+                          dict(N=2, nel=10, rot=2), 0.01),
     # the manufactured-solution test (Testcase 1) at N = 4 (tests/test_gpu_convergence.py)
     "conv_tc1_N4": (lambda: problems.conv_test(N=4, nel=6), dict(cart=(0.0, 2.0, 0.0, 2.0, 6, 6, 0, 0)), 0.02),
     # an ensemble member at its own scales: 2000 km square, 4000 m shelf, Okada uplift, viscosity on
