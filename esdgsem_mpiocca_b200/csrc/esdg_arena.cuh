@@ -158,6 +158,10 @@ class Arena : public Engine {
                     return bad("element tables out of range");
                 sd[k] = make_int4(fc + rf.begin, MS_h[k], OR_h[k], 0);
             }
+        if (pack_face_flags(ft, sd, re.begin, rf.begin)) {
+            give(free_e, re); give(free_f, rf);
+            return ESDG_E_ARG;
+        }
         const size_t eo = (size_t)re.begin, fo = (size_t)rf.begin;
         int r = 0;
         if ((r = h2d(nx + fo * ngl, nx_h, nf, "nx")) || (r = h2d(ny + fo * ngl, ny_h, nf, "ny")) ||

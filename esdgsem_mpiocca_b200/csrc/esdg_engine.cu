@@ -257,7 +257,7 @@ class Engine {
             (r = alloc(&GLw, (size_t)ngl)) || (r = alloc(&EleSizes, (size_t)K)))
             return r;
         if ((r = alloc(&nx, nf)) || (r = alloc(&ny, nf)) || (r = alloc(&scal, nf)) || (r = alloc(&bL, nf)) ||
-            (r = alloc(&bR, nf)) || (r = alloc(&SP, nf * 3)))
+            (r = alloc(&bR, nf)) || (r = alloc(&SP, (size_t)K * 12 * ngl)))
             return r;
         if ((r = alloc(&EdgeData, (size_t)F * 8)) || (r = alloc(&ftab, (size_t)F)) || (r = alloc(&side, (size_t)K * 4)))
             return r;
@@ -309,6 +309,7 @@ class Engine {
         // Validate the connectivity on the host, so that no kernel can index
         // outside its buffers.
         if (!MS_h || !OR_h || !E2E_h || !ED_h || !ER_h) return fail(ESDG_E_ARG, "null connectivity table");
+        int r = 0;
         std::vector<int4> ft(F), sd((size_t)K * 4);
         for (int f = 0; f < F; ++f) {
             const int* r = ED_h + (size_t)f * 8;
@@ -334,7 +335,7 @@ class Engine {
                 if (orr != 0 && orr != 1) return fail(ESDG_E_ARG, "ElemEdgeOrientation must be 0/1");
                 sd[id] = make_int4(fc, ms, orr, 0);
             }
-        int r = 0;
+        if ((r = pack_face_flags(ft, sd))) return r;
         if ((r = h2d(nx, nx_h, nf, "normalsX")) || (r = h2d(ny, ny_h, nf, "normalsY")) ||
             (r = h2d(scal, scal_h, nf, "Scal")) || (r = h2d(Yxi, yxi_h, nn, "y_xi")) ||
             (r = h2d(Yeta, yeta_h, nn, "y_eta")) || (r = h2d(Xxi, xxi_h, nn, "x_xi")) ||
@@ -356,6 +357,30 @@ class Engine {
         Vinv_h.assign(Vinv_h_, Vinv_h_ + n2);
         Dfd_h.assign(D_h, D_h + n2);
         copied = true;
+        return 0;
+    }
+
+    // Checks that the face records and the element side table describe the
+    // same sides (ElemToEdge[e][s] is the face whose record names (e, s)) and
+    // packs each face's element-side flags (orientation and MasterSlave of
+    // both sides, face_side_flags) into ft[f].w for the face kernel, which
+    // writes every face's flux into its elements' side slots.  ft and sd are
+    // in one numbering (a single mesh, or one arena instance's ranges).
+    int pack_face_flags(std::vector<int4>& ft, const std::vector<int4>& sd, int e_base = 0, int f_base = 0) {
+        for (size_t f = 0; f < ft.size(); ++f) {
+            int4& t = ft[f];
+            const int eL = t.x - e_base, sL = t.z & 3, eR = t.y < 0 ? -1 : t.y - e_base, sR = (t.z >> 2) & 3;
+            const int4 l = sd[(size_t)eL * 4 + sL];
+            if (l.x - f_base != (int)f) return fail(ESDG_E_ARG, "ElemToEdge of a face's left side names another face");
+            int oR = 0, mR = 1;
+            if (eR >= 0) {
+                const int4 rr = sd[(size_t)eR * 4 + sR];
+                if (rr.x - f_base != (int)f)
+                    return fail(ESDG_E_ARG, "ElemToEdge of a face's right side names another face");
+                oR = rr.z; mR = rr.y;
+            }
+            t.w = face_side_flags(l.z, l.y, oR, mR);
+        }
         return 0;
     }
 
@@ -1778,16 +1803,18 @@ static void noalloc_launch(int K, int F, int NumFlux, const PhysConst& c, const 
                 base + L.SP, nullptr, nullptr, nullptr, st, c};
     const long nfn = (long)F * NGL;
     const int fb = (int)((nfn + 255) / 256);
-    if (NumFlux == 0) k_face_flux<NGL, 0, false><<<fb, 256, 0, s>>>(fa);
-    else if (NumFlux == 2) k_face_flux<NGL, 2, false><<<fb, 256, 0, s>>>(fa);
-    else k_face_flux<NGL, 3, false><<<fb, 256, 0, s>>>(fa);
+    // face-major fluxes with the side table (SIDEOUT / SIDEIN off): the
+    // scratch layout of this entry point
+    if (NumFlux == 0) k_face_flux<NGL, 0, false, false, false><<<fb, 256, 0, s>>>(fa);
+    else if (NumFlux == 2) k_face_flux<NGL, 2, false, false, false><<<fb, 256, 0, s>>>(fa);
+    else k_face_flux<NGL, 3, false, false, false><<<fb, 256, 0, s>>>(fa);
     ElemArgs ea;
     memset(&ea, 0, sizeof ea);
     ea.K = K; ea.Jinv = Jinv; ea.Yxi = Yxi; ea.Yeta = Yeta; ea.Xxi = Xxi; ea.Xeta = Xeta; ea.Bx = Bx; ea.By = By;
     ea.D = D; ea.SP = base + L.SP; ea.side = reinterpret_cast<const int4*>(base + L.side);
     ea.q = const_cast<double*>(q); ea.Qt = Qt; ea.st = st; ea.mode = 2; ea.c = c;
     using S = ElemShape<NGL>;
-    k_element<NGL><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, s>>>(ea);
+    k_element<NGL, false><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, s>>>(ea);
 }
 
 static std::mutex g_noalloc_mu;

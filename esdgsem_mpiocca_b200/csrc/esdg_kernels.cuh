@@ -39,16 +39,35 @@ struct DevState {
     int pause_on, resume_steps;
 };
 
+// Element-side face fluxes (the SP buffer of the engine): for side s of
+// element e, the scaled ES flux of that side's face at the side's own nodes
+// j = 0..NGL-1 (the element's orientation of the side), already multiplied
+// by -MasterSlave: SP[((e * 4 + s) * 3 + eq) * NGL + j].  The element then
+// adds fs * Jinv, which is the reference's -ms * flux * Jinv
+// (okl/DG/SurfaceKernel.okl:17-142) bit for bit (the sign flip is exact),
+// and bulk-copies its tile's fluxes with the rest of the tile.
+__host__ __device__ __forceinline__ long side_flux_at(int e, int side, int eq, int j, int ngl) {
+    return ((long)(e * 4 + side) * 3 + eq) * ngl + j;
+}
+
+// Packed face record: x elemL, y elemR or -1, z sideL | sideR << 2 |
+// sameOrient << 4, w the element-side flags the face kernel needs to write
+// element-side fluxes: orientation of the left side (bit 0), its
+// MasterSlave == -1 (bit 1), the same two for the right side (bits 2, 3).
+__host__ __device__ __forceinline__ int face_side_flags(int orientL, int msL, int orientR, int msR) {
+    return (orientL ? 1 : 0) | (msL < 0 ? 2 : 0) | (orientR ? 4 : 0) | (msR < 0 ? 8 : 0);
+}
+
 struct FaceArgs {
     int F;
-    const int4* __restrict__ ftab;  // (elemL, elemR or -1, sideL | sideR<<2 | sameOrient<<4, 0)
+    const int4* __restrict__ ftab;  // (elemL, elemR or -1, sideL | sideR<<2 | sameOrient<<4, side flags)
     const double* __restrict__ q;
     const double* __restrict__ nx;
     const double* __restrict__ ny;
     const double* __restrict__ scal;
     const double* __restrict__ bL;
     const double* __restrict__ bR;
-    double* __restrict__ SP;   // [F][3][ngl]
+    double* __restrict__ SP;   // element-side fluxes [K][4][3][ngl] (face-major [F][3][ngl] without SIDEOUT)
     double* __restrict__ SGX;  // [F][2][ngl] (AV only)
     double* __restrict__ SGY;
     const int* __restrict__ elem_inst;
@@ -82,7 +101,7 @@ struct ElemArgs {
     const double* __restrict__ Dhat;    // BR1 gradient matrix
     const double* __restrict__ Dstrong; // viscous volume matrix
     const double* __restrict__ Vinv;    // modal transform
-    const double* __restrict__ SP;      // face fluxes [F][3][ngl]
+    const double* __restrict__ SP;      // element-side face fluxes [K][4][3][ngl] (see side_flux_at)
     const double* __restrict__ SGX;     // gradient face fluxes [F][2][ngl]
     const double* __restrict__ SGY;
     const double* __restrict__ SPV;     // viscous face fluxes [F][2][ngl]
@@ -145,7 +164,7 @@ __device__ __forceinline__ int inst_of(const int* elem_inst, int e) { return ele
 // Face kernel.
 // ---------------------------------------------------------------------------
 // One face node (gid = face * NGL + node) of the face kernel.
-template <int NGL, int NUMFLUX, bool AV>
+template <int NGL, int NUMFLUX, bool AV, bool SIDEOUT>
 __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
     const int f = (int)(gid / NGL), i = (int)(gid % NGL);
     constexpr int N2 = NGL * NGL;
@@ -188,10 +207,27 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
     double N0, N1, N2f;
     es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, bLx, a.bR[(long)f * NGL + ir], N0, N1, N2f);
     const double s = sc;
-    double* sp = a.SP + (long)f * 3 * NGL + i;
-    sp[0] = s * a.c.geomFace * N0;
-    sp[NGL] = s * a.c.geomFace * N1;
-    sp[2 * NGL] = s * a.c.geomFace * N2f;
+    const double v0 = s * a.c.geomFace * N0, v1 = s * a.c.geomFace * N1, v2 = s * a.c.geomFace * N2f;
+    if (SIDEOUT) {
+        // both sides' copies, each in its element's node order and signed
+        // by -MasterSlave (side_flux_at)
+        const int w = t.w;
+        const int jL = (w & 1) ? i : NGL - 1 - i;
+        double* pl = a.SP + side_flux_at(eL, sL, 0, jL, NGL);
+        const bool nL = (w & 2) != 0;
+        pl[0] = nL ? v0 : -v0; pl[NGL] = nL ? v1 : -v1; pl[2 * NGL] = nL ? v2 : -v2;
+        if (eR >= 0) {
+            const int jR = (w & 4) ? i : NGL - 1 - i;
+            double* pr = a.SP + side_flux_at(eR, sR, 0, jR, NGL);
+            const bool nR = (w & 8) != 0;
+            pr[0] = nR ? v0 : -v0; pr[NGL] = nR ? v1 : -v1; pr[2 * NGL] = nR ? v2 : -v2;
+        }
+    } else {
+        double* sp = a.SP + (long)f * 3 * NGL + i;
+        sp[0] = v0;
+        sp[NGL] = v1;
+        sp[2 * NGL] = v2;
+    }
     if (grad) {
         // okl/BR1_Gradient/calcNumFluxesGradient.okl:16-135 (the right trace
         // is taken in the right element's own order, as there).
@@ -212,16 +248,18 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
 // grid).  STRIDE = true: a resident grid strides over the face nodes below
 // the live extent (an arena, whose face capacity can be far above its live
 // faces); a separate instantiation, since the loop costs registers.
-template <int NGL, int NUMFLUX, bool AV, bool STRIDE = false>
+// SIDEOUT = true: element-side fluxes (the engine); false: the face-major
+// [F][3][ngl] layout of the allocation-free entry point.
+template <int NGL, int NUMFLUX, bool AV, bool STRIDE = false, bool SIDEOUT = true>
 __global__ void __launch_bounds__(256, STRIDE ? 4 : 1) k_face_flux(FaceArgs a) {
     long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long all = (long)a.F * NGL;
     if (!STRIDE) {
         if (gid >= all || (a.extent && gid >= (long)a.extent[1] * NGL)) return;
-        face_flux_node<NGL, NUMFLUX, AV>(a, gid);
+        face_flux_node<NGL, NUMFLUX, AV, SIDEOUT>(a, gid);
     } else {
         const long n = a.extent ? min(all, (long)a.extent[1] * NGL) : all;
-        for (; gid < n; gid += (long)gridDim.x * blockDim.x) face_flux_node<NGL, NUMFLUX, AV>(a, gid);
+        for (; gid < n; gid += (long)gridDim.x * blockDim.x) face_flux_node<NGL, NUMFLUX, AV, SIDEOUT>(a, gid);
     }
 }
 
@@ -337,7 +375,9 @@ __device__ __forceinline__ double node_lambda(const PhysConst& c, double h, doub
 // okl/DG/VolumeKernelFluxDiffV99.okl:60-218, okl/DG/SurfaceKernel.okl:17-142,
 // okl/RungeKutta/rkLS.okl:17-89 + UpdateKernelLS.okl:17-78 (mode 0),
 // okl/RungeKutta/UpdateKernelSSP_V1.okl:17-98 (mode 1).
-template <int NGL>
+// SIDEIN = true: element-side fluxes (the engine); false: face-major fluxes
+// with the side table (the allocation-free entry point).
+template <int NGL, bool SIDEIN = true>
 __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a) {
     constexpr int N2 = NGL * NGL, NE = ElemShape<NGL>::NE;
     __shared__ double sD[N2];
@@ -360,8 +400,8 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
     // partners), Jinv/Bx/By, gRK (or Qtmp) and the face fluxes of the
     // node's sides.
     double h = 0, hu = 0, hv = 0, J = 0, bx = 0, by = 0, o0 = 0, o1 = 0, o2 = 0, dt = 0;
-    double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    int ms[2] = {0, 0};
+    double f[2][3] = {{0, 0, 0}, {0, 0, 0}};  // signed side fluxes, -ms * flux
+    bool has[2] = {false, false};
     const bool to_list = active && a.act && a.act[e] != 0;
     if (active) {
         h = a.q[qid]; hu = a.q[qid + N2]; hv = a.q[qid + 2 * N2];
@@ -382,11 +422,17 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
                 else if (xi == 0) { side = 3; j = eta; }
             }
             if (side >= 0) {
-                const int4 sd = a.side[(long)e * 4 + side];
-                const int inc = sd.z ? j : NGL - 1 - j;
-                const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
-                ms[pass] = sd.y;
-                f[pass][0] = fp[0]; f[pass][1] = fp[NGL]; f[pass][2] = fp[2 * NGL];
+                has[pass] = true;
+                if (SIDEIN) {
+                    const double* fp = a.SP + side_flux_at(e, side, 0, j, NGL);
+                    f[pass][0] = fp[0]; f[pass][1] = fp[NGL]; f[pass][2] = fp[2 * NGL];
+                } else {
+                    const int4 sd = a.side[(long)e * 4 + side];
+                    const int inc = sd.z ? j : NGL - 1 - j;
+                    const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
+                    const double m = -sd.y;
+                    f[pass][0] = m * fp[0]; f[pass][1] = m * fp[NGL]; f[pass][2] = m * fp[2 * NGL];
+                }
             }
         }
         si[s] = (h > 0) ? 1.0 / h : 0.0;
@@ -425,11 +471,10 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element(ElemArgs a)
         const double db = 0.0;
 #pragma unroll
         for (int pass = 0; pass < 2; ++pass) {
-            if (ms[pass] != 0) {
-                const int m = ms[pass];
-                r0 += -m * f[pass][0] * J;
-                r1 += -m * J * f[pass][1] + J * db;
-                r2 += -m * J * f[pass][2] + J * db;
+            if (has[pass]) {
+                r0 += f[pass][0] * J;
+                r1 += J * f[pass][1] + J * db;
+                r2 += J * f[pass][2] + J * db;
             }
         }
         if (a.conv) add_conv_source(a, a.st[ins], xid, bx, by, r0, r1, r2);
@@ -600,12 +645,12 @@ __global__ void __launch_bounds__(ElemShape<NGL>::THREADS) k_element_av1(ElemArg
             if (side >= 0) {
                 const int4 sd = a.side[(long)e * 4 + side];
                 const int inc = sd.z ? j : NGL - 1 - j;
-                const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
+                const double* fp = a.SP + side_flux_at(e, side, 0, j, NGL);
                 const int ms = sd.y;
                 const double db = 0.0;
-                r0 += -ms * fp[0] * J;
-                r1 += -ms * J * fp[NGL] + J * db;
-                r2 += -ms * J * fp[2 * NGL] + J * db;
+                r0 += fp[0] * J;
+                r1 += J * fp[NGL] + J * db;
+                r2 += J * fp[2 * NGL] + J * db;
                 const double* ux = a.SGX + (long)sd.x * 2 * NGL + inc;
                 const double* uy = a.SGY + (long)sd.x * 2 * NGL + inc;
                 if (pass == 0) gx0 += ms * ux[0] * J;

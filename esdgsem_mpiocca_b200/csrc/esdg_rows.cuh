@@ -15,7 +15,8 @@
 // its eta terms, again in partner order.
 //
 // Per tile of NE elements one thread issues ten 1-D bulk copies (q, gRK or
-// Qtmp, Jinv, Bx, By, Y_xi, Y_eta, X_xi, X_eta, the side table) into the
+// Qtmp, Jinv, Bx, By, Y_xi, Y_eta, X_xi, X_eta, the element-side face
+// fluxes) into the
 // stage's buffer; the updated q (and gRK) are written back into the same
 // buffer and leave with one bulk store per array when every element of the
 // tile is active and none is partly dry, by plain stores otherwise.  Thread
@@ -47,8 +48,8 @@ struct RowShape {
     static constexpr int THREADS = (LINES + 31) / 32 * 32;
     static constexpr int QD = 3 * NE * N2;
     static constexpr int ND = NE * N2;
-    static constexpr int SIDE_D = NE * 8;  // 4 int4 side entries per element
-    static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND + SIDE_D;
+    static constexpr int FD = NE * 12 * NGL;  // element-side face fluxes of the tile
+    static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND + FD;
     // shared layout: [ST][stage] | xi sums [3][ND] | mbar[ST]
     static constexpr size_t SMEM = sizeof(double) * ((size_t)ST * STAGE_DOUBLES + 3 * (size_t)ND) + 16 * ST;
 };
@@ -56,7 +57,8 @@ struct RowShape {
 // Elements per tile of the row kernel's variants: the largest of 32 (64
 // for NGL = 2) that keeps two stages within 200 KB, and half of it.
 __host__ __device__ constexpr size_t row_smem_bytes(int ngl, int ne, int st) {
-    return sizeof(double) * ((size_t)st * (size_t)ne * (13 * ngl * ngl + 8) + 3 * (size_t)ne * ngl * ngl) + 16 * st;
+    return sizeof(double) * ((size_t)st * (size_t)ne * (13 * ngl * ngl + 12 * ngl) + 3 * (size_t)ne * ngl * ngl) +
+           16 * st;
 }
 __host__ __device__ constexpr int row_ne_fit(int ngl, int ne) {
     return (ne <= 2 || row_smem_bytes(ngl, ne, 2) <= 200 * 1024) ? ne : row_ne_fit(ngl, ne - 2);
@@ -89,10 +91,10 @@ __device__ __forceinline__ void rows_issue_tile(const ElemArgs& a, int t, double
     const int ne = min(NE, a.K - e0);
     const unsigned qb = (unsigned)(ne * 3 * S::N2 * sizeof(double));
     const unsigned nb = (unsigned)(ne * S::N2 * sizeof(double));
-    const unsigned sbytes = (unsigned)(ne * 4 * sizeof(int4));
+    const unsigned fbytes = (unsigned)(ne * 12 * NGL * sizeof(double));
     const double* second = (a.mode == 1) ? a.Qtmp : a.gRK;
     const bool need2 = a.mode != 2;
-    mbar_arrive_expect_tx(bar, qb + (need2 ? qb : 0u) + 7u * nb + sbytes);
+    mbar_arrive_expect_tx(bar, qb + (need2 ? qb : 0u) + 7u * nb + fbytes);
     const long qo = (long)e0 * 3 * S::N2, no = (long)e0 * S::N2;
     bulk_g2s(sb, a.q + qo, qb, bar);
     if (need2) bulk_g2s(sb + S::QD, second + qo, qb, bar);
@@ -104,7 +106,7 @@ __device__ __forceinline__ void rows_issue_tile(const ElemArgs& a, int t, double
     bulk_g2s(nd + 4 * S::ND, a.Yeta + no, nb, bar);
     bulk_g2s(nd + 5 * S::ND, a.Xxi + no, nb, bar);
     bulk_g2s(nd + 6 * S::ND, a.Xeta + no, nb, bar);
-    bulk_g2s(nd + 7 * S::ND, a.side + (long)e0 * 4, sbytes, bar);
+    bulk_g2s(nd + 7 * S::ND, a.SP + side_flux_at(e0, 0, 0, 0, NGL), fbytes, bar);
 }
 
 // Flux-differencing sums along one line of NGL nodes held in registers
@@ -201,7 +203,7 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
         const double* sYe = sJ + 4 * ND;
         const double* sXx = sJ + 5 * ND;
         const double* sXe = sJ + 6 * ND;
-        const int4* sSide = reinterpret_cast<const int4*>(sJ + 7 * ND);
+        const double* sF = sJ + 7 * ND;  // element-side face fluxes [NE][4][3][NGL]
         const int e0 = t * NE;
         const int e = e0 + el;
         const bool inb = worker && e < a.K;
@@ -246,32 +248,12 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
         double lam = 0.0;
         if (active) {
             const int qc = el * 3 * N2 + ln, nc = el * N2 + ln;
-            // face fluxes of the column's boundary nodes (global, mostly L2),
-            // requested before the arithmetic: sides 0 (j = 0) and 2
-            // (j = NGL-1) in eta, 1 (ln = NGL-1) or 3 (ln = 0) in xi
-            const int4* sides = sSide + el * 4;
-            const int4 a0 = sides[0], a2 = sides[2];
+            // the column's boundary nodes take the element-side fluxes
+            // (-ms * flux) of sides 0 (j = 0) and 2 (j = NGL-1) in eta, 1
+            // (ln = NGL-1) or 3 (ln = 0) in xi
+            const double* fel = sF + el * 12 * NGL;
             const bool xedge = (ln == 0) || (ln == NGL - 1);
-            double fe[2][3], fx[NGL][3];
-            int mx = 0;
-            {
-                const double* p0 = a.SP + (long)a0.x * 3 * NGL + (a0.z ? ln : NGL - 1 - ln);
-                const double* p2 = a.SP + (long)a2.x * 3 * NGL + (a2.z ? ln : NGL - 1 - ln);
-                fe[0][0] = p0[0]; fe[0][1] = p0[NGL]; fe[0][2] = p0[2 * NGL];
-                fe[1][0] = p2[0]; fe[1][1] = p2[NGL]; fe[1][2] = p2[2 * NGL];
-#pragma unroll
-                for (int j = 0; j < NGL; ++j) fx[j][0] = fx[j][1] = fx[j][2] = 0.0;
-                if (xedge) {
-                    const int4 ax = sides[ln == NGL - 1 ? 1 : 3];
-                    mx = ax.y;
-                    const double* px = a.SP + (long)ax.x * 3 * NGL;
-#pragma unroll
-                    for (int j = 0; j < NGL; ++j) {
-                        const int inc = ax.z ? j : NGL - 1 - j;
-                        fx[j][0] = px[inc]; fx[j][1] = px[inc + NGL]; fx[j][2] = px[inc + 2 * NGL];
-                    }
-                }
-            }
+            const double* fx = fel + (ln == NGL - 1 ? 1 : 3) * 3 * NGL;
             double h[NGL], hu[NGL], hv[NGL], u[NGL], v[NGL], h2[NGL], yx[NGL], xx[NGL];
             line_load<NGL>(sq, sYx, sXx, qc, nc, NGL, h, hu, hv, u, v, h2, yx, xx);
             double d1[NGL], d2[NGL], d3[NGL];
@@ -298,19 +280,16 @@ __global__ void __launch_bounds__(RowShape<NGL, NE, ST>::THREADS, MINB)
                     pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sq + el * 3 * N2, a.Bn + (long)e * N2, j, ln, sYe[s],
                                    sYx[s], sXe[s], sXx[s], J, r1, r2);
                 const double db = 0.0;
-                if (j == 0 || j == NGL - 1) {  // eta sides (0 at j = 0, 2 at j = NGL-1)
-                    const int m = (j == 0) ? a0.y : a2.y;
-                    const double* f = fe[j == 0 ? 0 : 1];
-                    if (m != 0) {
-                        r0 += -m * f[0] * J;
-                        r1 += -m * J * f[1] + J * db;
-                        r2 += -m * J * f[2] + J * db;
-                    }
+                if (j == 0 || j == NGL - 1) {  // eta sides (0 at j = 0, 2 at j = NGL-1), node ln along them
+                    const double* f = fel + (j == 0 ? 0 : 2) * 3 * NGL + ln;
+                    r0 += f[0] * J;
+                    r1 += J * f[NGL] + J * db;
+                    r2 += J * f[2 * NGL] + J * db;
                 }
-                if (xedge && mx != 0) {  // xi side (1 at ln = NGL-1, 3 at ln = 0)
-                    r0 += -mx * fx[j][0] * J;
-                    r1 += -mx * J * fx[j][1] + J * db;
-                    r2 += -mx * J * fx[j][2] + J * db;
+                if (xedge) {  // xi side (1 at ln = NGL-1, 3 at ln = 0), node j along it
+                    r0 += fx[j] * J;
+                    r1 += J * fx[NGL + j] + J * db;
+                    r2 += J * fx[2 * NGL + j] + J * db;
                 }
                 if (a.conv) add_conv_source(a, a.st[ins], (long)e * N2 + j * NGL + ln, sBx[s], sBy[s], r0, r1, r2);
                 const long qid = qe + j * NGL;

@@ -2,12 +2,13 @@
 // persistent, double-buffered element kernel built on them.
 //
 // Each CTA walks tiles of NE consecutive elements (tile = blockIdx.x,
-// blockIdx.x + gridDim.x, ...).  One thread issues, per tile, nine 1-D bulk
+// blockIdx.x + gridDim.x, ...).  One thread issues, per tile, ten 1-D bulk
 // copies global -> shared (q, gRK or Qtmp, Jinv, Bx, By, Y_xi, Y_eta, X_xi,
-// X_eta: all contiguous in the element-major layout) completing on the
-// stage's mbarrier; while the CTA computes tile k the copies of tile k+1 are
-// in flight.  The arithmetic per node is that of k_element (same operands,
-// same order), only the staging differs.
+// X_eta and the element-side face fluxes: all contiguous in the
+// element-major layout) completing on the stage's mbarrier; while the CTA
+// computes tile k the copies of tile k+1 are in flight.  The arithmetic per
+// node is that of k_element (same operands, same order), only the staging
+// differs: no load of the compute phase leaves the shared memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -134,7 +135,8 @@ struct TmaShape {
     static constexpr int STAGES = ST;
     static constexpr int QD = NE * 3 * N2;  // doubles of a q-like section
     static constexpr int ND = NE * N2;      // doubles of a nodal section
-    static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND;
+    static constexpr int FD = NE * 12 * NGL;  // element-side face fluxes of the tile
+    static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND + FD;
     // shared layout: [STAGES][stage] | su, sv, sh2 [ND each] | sD[N2] | mbar[STAGES]
     static constexpr size_t SMEM = sizeof(double) * (STAGES * (size_t)STAGE_DOUBLES + 3 * ND + N2) + 16 * STAGES;
 };
@@ -148,10 +150,12 @@ __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double*
     const int ne = min(S::NE, a.K - e0);
     const unsigned qb = (unsigned)(ne * 3 * S::N2 * sizeof(double));
     const unsigned nb = (unsigned)(ne * S::N2 * sizeof(double));
+    const unsigned fb = (unsigned)(ne * 12 * NGL * sizeof(double));
     const double* second = (a.mode == 1) ? a.Qtmp : a.gRK;
     const bool need2 = a.mode != 2;
-    mbar_arrive_expect_tx(bar, qb + (need2 ? qb : 0u) + 7u * nb);
+    mbar_arrive_expect_tx(bar, qb + (need2 ? qb : 0u) + 7u * nb + fb);
     const long qo = (long)e0 * 3 * S::N2, no = (long)e0 * S::N2;
+    bulk_g2s(sb + 2 * S::QD + 7 * S::ND, a.SP + side_flux_at(e0, 0, 0, 0, NGL), fb, bar);
     bulk_g2s(sb, a.q + qo, qb, bar);
     if (need2) bulk_g2s(sb + S::QD, second + qo, qb, bar);
     double* nd = sb + 2 * S::QD;
@@ -210,31 +214,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
         const int ins = inb ? inst_of(a.elem_inst, e) : 0;
         const bool active = inb && !a.st[ins].done;
         const bool to_list = active && a.act && a.act[e] != 0;
-        // face fluxes of this node's sides (global, mostly L2) before the wait
-        double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
-        int ms[2] = {0, 0};
-        double dt = 0.0;
-        if (active) {
-            if (a.mode != 2) dt = a.st[ins].dt;
-#pragma unroll
-            for (int pass = 0; pass < 2; ++pass) {
-                int side = -1, j = 0;
-                if (pass == 0) {
-                    if (eta == 0) { side = 0; j = xi; }
-                    else if (eta == NGL - 1) { side = 2; j = xi; }
-                } else {
-                    if (xi == NGL - 1) { side = 1; j = eta; }
-                    else if (xi == 0) { side = 3; j = eta; }
-                }
-                if (side >= 0) {
-                    const int4 sd = a.side[(long)e * 4 + side];
-                    const int inc = sd.z ? j : NGL - 1 - j;
-                    const double* fp = a.SP + (long)sd.x * 3 * NGL + inc;
-                    ms[pass] = sd.y;
-                    f[pass][0] = fp[0]; f[pass][1] = fp[NGL]; f[pass][2] = fp[2 * NGL];
-                }
-            }
-        }
+        const double dt = (active && a.mode != 2) ? a.st[ins].dt : 0.0;
         // every thread waits for the tile; a copy that never lands makes the
         // whole CTA leave together (uniform decision) with an error status
         // for the host instead of hanging
@@ -293,14 +273,25 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
             if (a.dry && a.dry[e])
                 pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sq + el * 3 * N2, a.Bn + (long)e * N2, eta, xi, ye, yx, xe, xx,
                                J, r1, r2);
+            // lift: sides 0/2 first, then 1/3, from the tile's element-side
+            // fluxes (-ms * flux; DBSurf1/2 are zero)
             const double db = 0.0;
+            const double* sF = sJ + 7 * S::ND + el * 12 * NGL;
 #pragma unroll
             for (int pass = 0; pass < 2; ++pass) {
-                if (ms[pass] != 0) {
-                    const int m = ms[pass];
-                    r0 += -m * f[pass][0] * J;
-                    r1 += -m * J * f[pass][1] + J * db;
-                    r2 += -m * J * f[pass][2] + J * db;
+                int side = -1, j = 0;
+                if (pass == 0) {
+                    if (eta == 0) { side = 0; j = xi; }
+                    else if (eta == NGL - 1) { side = 2; j = xi; }
+                } else {
+                    if (xi == NGL - 1) { side = 1; j = eta; }
+                    else if (xi == 0) { side = 3; j = eta; }
+                }
+                if (side >= 0) {
+                    const double* fp = sF + side * 3 * NGL + j;
+                    r0 += fp[0] * J;
+                    r1 += J * fp[NGL] + J * db;
+                    r2 += J * fp[2 * NGL] + J * db;
                 }
             }
             if (a.conv) add_conv_source(a, a.st[ins], (long)e * N2 + nd, sBx[s], sBy[s], r0, r1, r2);
