@@ -45,7 +45,8 @@ def log(*a):
 
 # element-kernel variants of the engine at N = 4 (index = variant number)
 ELEMENT_KERNELS_N4 = ("k_element_tma<5,2,2>", "k_element_tma<5,3,2>", "k_element_tma<5,2,3>",
-                      "k_element_rows<5,32,2,1>", "k_element_rows<5,16,2,2>")
+                      "k_element_rows<5,30,2,1>", "k_element_rows<5,14,2,2>", "k_element_pair<5,3>",
+                      "k_element_pair<5,4>")
 
 
 def element_kernel_name(dc):
@@ -291,6 +292,8 @@ def main():
     ap.add_argument("--max-live-nodes", type=float, default=4e6,
                     help="serving workload, shortest-job-first run: nodes in flight at most")
     ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--indicator-schedule", default="stage", choices=["stage", "step"],
+                    help="ensemble workload: the learned indicator at every RK stage or once per step")
     ap.add_argument("--alone-members", type=int, default=15,
                     help="ensemble workload: members solved one at a time for the plain-path rate")
     args = ap.parse_args()
@@ -373,11 +376,12 @@ def main():
     # ensemble, batched with the learned indicator vs one at a time plain ----
     if not args.no_ensemble:
         line["batched_learned"] = ensemble_measure(256, args.ensemble_steps, 3, 10, local, dist, ws, rank,
-                                                   attribution=False)
+                                                   attribution=False, every_stage=True)
         line["batched_learned"]["workload"] = (
             "ensemble of 256 seeded tsunami members per GPU, N=3, K in {64..256}^2 on 2000 km squares, shelf, "
-            "seamounts, Okada uplift, artificial viscosity; batched arena with the learned indicator and the "
-            f"active set vs 10 members (every size class) one at a time on the plain path; "
+            "seamounts, Okada uplift, artificial viscosity; batched arena with the learned indicator (every RK "
+            "stage, as the reference's sensor) and the active set vs 10 members (every size class) one at a "
+            "time on the plain path; "
             f"{args.ensemble_steps} LS-RK4 steps after 3 warm-up steps (the configuration runs 500)")
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(os.cpu_count() or 1, args.steps, args.warmup, prob=prob)[0]
@@ -448,7 +452,8 @@ def _alone_sample(seeds, k):
     return out
 
 
-def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank, attribution=True):
+def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank, attribution=True,
+                     every_stage=False):
     """The ensemble configuration: seeded tsunami members (N=3, K in
     {64..256}^2 on 2000 km squares, artificial viscosity) advanced in one
     arena with the learned indicator and the active set, against the plain
@@ -460,6 +465,8 @@ def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank,
     the learned and the modal viscosity flags on the plain solutions' final
     states, the indicator's decision shares, the clocks of the timed region
     and, with `attribution`, the batched rates of the other indicator modes.
+    The learned indicator runs once per step (every_stage=False; its
+    viscosity and active set kept for the step's stages) or at every stage.
     Per-step work: src/deviceclass.cpp:897-1130 for every member."""
     import torch
     from esdgsem_mpiocca_b200 import problems
@@ -478,11 +485,12 @@ def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank,
                    ArtificialViscosity=p0.ArtificialViscosity, epsilon_0=p0.epsilon_0,
                    sigma_max=p0.sigma_max, sigma_min=p0.sigma_min, device_id=local)
     ens.set_indicator(2, net)
+    ens.set_indicator_every_stage(every_stage)
     t0 = time.perf_counter()
     dofs, ids, kept = 0, {}, {}
     for sd in seeds:
         pr = problems.tsunami_member(sd)
-        ids[sd] = ens.add(pr, T=1e9, max_steps=total + (2 * attr_steps if attribution else 0))
+        ids[sd] = ens.add(pr, T=1e9, max_steps=total + (3 * attr_steps if attribution else 0))
         dofs += pr.dofs()
         if sd in sample:
             kept[sd] = pr
@@ -520,7 +528,10 @@ def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank,
     learned["all_done"] = all(x == total for x in learned["steps"])
     qb = {sd: ens.q(ids[sd]) for sd in sample}
     attrib = {}
-    if attribution:  # the same arena continued with the other indicator modes
+    if attribution:  # the same arena continued with the other schedule and indicator modes
+        ens.set_indicator_every_stage(not every_stage)
+        attrib["other_schedule"] = timed(attr_steps)
+        ens.set_indicator_every_stage(every_stage)
         for m in (0, 1):
             ens.set_indicator(m)
             attrib[m] = timed(attr_steps)
@@ -568,11 +579,15 @@ def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank,
            "max_rel_l2_deviation_vs_plain": dev,
            "flag_agreement": agree / max(nflag, 1),
            "indicator": {"network_settled": decided / max(evals, 1), "modal_fallback": stt["modal"] / max(evals, 1),
-                         "viscous_share": stt["viscous"] / max(evals, 1), "margin": net.margin},
+                         "viscous_share": stt["viscous"] / max(evals, 1), "margin": net.margin,
+                         "schedule": "every RK stage" if every_stage else "once per step (start of step)"},
            "gpu_launches": int(learned["launches"]), "clocks": learned["clocks"]}
     if attribution:
         out["attribution_batched"] = {"modal_full_path": attrib[0]["rate"], "modal_active_set": attrib[1]["rate"],
-                                      "learned_active_set": learned["rate"], "steps": attr_steps}
+                                      "learned_active_set": learned["rate"],
+                                      ("learned_every_stage" if not every_stage else "learned_once_per_step"):
+                                          attrib["other_schedule"]["rate"],
+                                      "steps": attr_steps}
     return out
 
 
@@ -585,7 +600,8 @@ def ensemble_bench(args):
     dist = init_dist(ws)
     steps = args.steps if args.steps != 20 else 500
     warm = max(args.warmup, 3)
-    r = ensemble_measure(args.members, steps, warm, args.alone_members, local, dist, ws, rank)
+    r = ensemble_measure(args.members, steps, warm, args.alone_members, local, dist, ws, rank,
+                         every_stage=args.indicator_schedule == "stage")
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": steps,
             "warmup": warm, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (indicator network: bf16 weights, fp32 accumulation)",
@@ -596,7 +612,8 @@ def ensemble_bench(args):
                        "members": r["members"], "nodes": r["nodes"], "setup_s": r["setup_s"],
                        "all_done": r["all_done"], "sharding": "members split across ranks, no exchange",
                        "members_with_error": r["members_with_error"],
-                       "l2": "state (~16 GB at 256 members) far larger than L2"}}
+                       "l2": "state (~16 GB at 256 members) far larger than L2",
+                       "indicator_schedule": args.indicator_schedule}}
     for k in ("plain_one_at_a_time", "ratio_batched_learned_over_plain", "max_rel_l2_deviation_vs_plain",
               "flag_agreement", "indicator", "attribution_batched", "gpu_launches", "clocks"):
         line[k] = r[k]

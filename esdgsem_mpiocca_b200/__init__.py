@@ -48,6 +48,11 @@ def _declare(lib):
         "esdg_profile_steps": (_I, [_VP, _I, _PD, _PD]),
         "esdg_debug_bulk_wait_test": (_I, [_VP, ctypes.c_longlong, _I]),
         "esdg_set_pause": (_I, [_VP, _D]),
+        "esdg_set_indicator_every_stage": (_I, [_VP, _I]),
+        "esdg_okada_uplift": (_I, [ctypes.c_longlong, _VP, _VP, _PD, _I, _I, _VP, _VP]),
+        "esdg_mesh_element_curves": (_I, [_VP, _PI, _PD, _PI, _PD]),
+        "esdg_geometry_device": (_I, [_I, _I, _I] + [_VP] * 13 + [_VP]),
+        "esdg_ensemble_set_indicator_every_stage": (_I, [_VP, _I]),
         "esdg_resume": (_I, [_VP, _PD, _PI]),
         "esdg_compute_rhs_noalloc": (_I, [_I, _I, _I, _I, _I, _D, _D] + [_VP] * 17 + [_VP, _VP]),
         "esdg_basis": (_I, [_I, _I] + [_PD] * 9),

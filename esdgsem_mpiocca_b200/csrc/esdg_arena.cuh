@@ -428,6 +428,12 @@ int esdg_ensemble_set_indicator(esdg_ensemble* en, int mode, const float* params
     return en->a.set_indicator(mode, params, nparams, margin);
 }
 
+int esdg_ensemble_set_indicator_every_stage(esdg_ensemble* en, int every_stage) {
+    if (!en) return ESDG_E_ARG;
+    cudaSetDevice(en->a.device);
+    return en->a.set_indicator_every_stage(every_stage);
+}
+
 int esdg_ensemble_indicator_stats(esdg_ensemble* en, unsigned long long* counts4, int reset) {
     if (!en || !counts4) return ESDG_E_ARG;
     cudaSetDevice(en->a.device);

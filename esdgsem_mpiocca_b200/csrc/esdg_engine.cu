@@ -29,8 +29,11 @@
 #include "esdg_kernels.cuh"
 #include "esdg_tma.cuh"
 #include "esdg_rows.cuh"
+#include "esdg_pair.cuh"
 #include "esdg_indicator.cuh"
 #include "esdg_analysis.cuh"
+#include "esdg_geometry.cuh"
+#include "esdg_okada.cuh"
 #include "esdg_setup.hpp"
 
 namespace esdg {
@@ -519,7 +522,8 @@ class Engine {
     // per SM, pipeline depth); then ROW_VARIANTS line-per-thread
     // k_element_rows (elements per tile).  The autotuner times them on the
     // mesh; esdg_set_element_variant can fix one.
-    static constexpr int ELEM_VARIANTS = TMA_VARIANTS + ROW_VARIANTS;
+    static constexpr int ELEM_VARIANTS = TMA_VARIANTS + ROW_VARIANTS + PAIR_VARIANTS;
+    static constexpr int PAIR_FIRST = TMA_VARIANTS + ROW_VARIANTS;  // two-nodes-per-thread variants follow
     int tma_grid[ELEM_VARIANTS] = {};  // persistent grid sizes (0: not usable)
     int tma_ctas[ELEM_VARIANTS] = {};  // resident CTAs per SM
     int tma_variant = 0;
@@ -562,6 +566,30 @@ class Engine {
         return 0;
     }
 
+    template <int NGL, int V>
+    int setup_pair_variant() {
+        using P = PairShape<NGL>;
+        auto kern = k_element_pair<NGL, pair_min_blocks(V)>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::THREADS, P::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+        const int ntiles = (K + P::NE - 1) / P::NE;
+        tma_grid[PAIR_FIRST + V] = per_sm > 0 ? std::max(1, std::min(ntiles, per_sm * sms)) : 0;
+        tma_ctas[PAIR_FIRST + V] = per_sm;
+        return 0;
+    }
+
+    template <int NGL, int V>
+    void launch_pair_v(const ElemArgs& ea) {
+        using P = PairShape<NGL>;
+        const int ntiles = (K + P::NE - 1) / P::NE;
+        k_element_pair<NGL, pair_min_blocks(V)><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
+    }
+
     template <int NGL>
     int setup_tma() {
         using T = TmaShape<NGL>;
@@ -577,6 +605,8 @@ class Engine {
             if (!r) r = setup_row_variant<NGL, 0>();
             if (!r) r = setup_row_variant<NGL, 1>();
         }
+        if (!r) r = setup_pair_variant<NGL, 0>();
+        if (!r) r = setup_pair_variant<NGL, 1>();
         return r;
     }
 
@@ -606,7 +636,9 @@ class Engine {
         else if (v == 1) launch_tma_v<NGL, 1>(ea);
         else if (v == 2) launch_tma_v<NGL, 2>(ea);
         else if (v == TMA_VARIANTS) launch_rows_v<NGL, 0>(ea);
-        else launch_rows_v<NGL, 1>(ea);
+        else if (v == TMA_VARIANTS + 1) launch_rows_v<NGL, 1>(ea);
+        else if (v == PAIR_FIRST) launch_pair_v<NGL, 0>(ea);
+        else launch_pair_v<NGL, 1>(ea);
     }
 
     template <int NGL>
@@ -710,7 +742,10 @@ class Engine {
             // step's dt), plain element kernel (flagged elements only write
             // Qt and are listed), then gradient, viscous face flux and
             // viscous update over the list
-            if (shock_stage) launch_indicator<NGL>(0);
+            if (shock_stage) {
+                if (ind_every_stage || indicator < 2) launch_indicator<NGL>(0);
+                else cudaMemsetAsync(act + K, 0, sizeof(int), stream);  // the step's flags, a new list
+            }
             launch_face<NGL>(true);
             ElemArgs ea = elem_args(mode, A, Bc, C, lam_in_elem);
             ea.act = act; ea.alist = alist; ea.acount = act + K;
@@ -820,6 +855,20 @@ class Engine {
             if (e != cudaSuccess) return cuda_fail(e, "occupancy (network)");
             mlp_grid = std::max(1, std::min(std::max(1, om) * sms, (K + 63) / 64));
         }
+        return 0;
+    }
+
+    // Schedule of the learned indicator (modes 2, 3): every stage, as the
+    // reference evaluates its sensor (src/deviceclass.cpp:1043-1046), or
+    // once per step, at the step start, the viscosity and the active set
+    // then kept for the step's stages.  Modes 0 and 1 (the modal sensor,
+    // exact) always run every stage.
+    bool ind_every_stage = true;
+
+    int set_indicator_every_stage(int every) {
+        if (!inited || !built) return fail(ESDG_E_ARG, "indicator schedule after buildDeviceKernels");
+        ind_every_stage = every != 0;
+        if (graph) return capture_step_graph();
         return 0;
     }
 
@@ -1236,8 +1285,10 @@ class Engine {
     void launch_rhs() {
         stage_tfrac = 0.0;  // one RHS at the state's own time
         if (AV) {
-            // the step-start sensor (shock_stage=1 recomputes it from q)
-            launch_stage<NGL>(2, 0.0, 0.0, 0.0, false, true);
+            // the sensor of this state (whatever the learned schedule), then
+            // the stage
+            launch_indicator<NGL>(0);
+            launch_stage<NGL>(2, 0.0, 0.0, 0.0, false, false);
         } else {
             launch_stage<NGL>(2, 0.0, 0.0, 0.0, false, false);
         }
@@ -1464,6 +1515,11 @@ int esdg_set_indicator(esdg_deviceclass* d, int mode, const float* params, int n
     return d->eng.set_indicator(mode, params, nparams, margin);
 }
 
+int esdg_set_indicator_every_stage(esdg_deviceclass* d, int every_stage) {
+    ESDG_GUARD(d);
+    return d->eng.set_indicator_every_stage(every_stage);
+}
+
 int esdg_indicator_stats(esdg_deviceclass* d, unsigned long long* counts4, int reset) {
     ESDG_GUARD(d);
     if (!counts4) return d->eng.fail(ESDG_E_ARG, "null counts");
@@ -1656,6 +1712,128 @@ int esdg_mesh_write_ism2(const esdg_mesh* m, const char* path) {
     } catch (const std::exception& ex) {
         esdg::g_create_error = ex.what();
         return ESDG_E_IO;
+    }
+    return ESDG_OK;
+}
+
+int esdg_mesh_element_curves(const esdg_mesh* m, int* curve_order, double* corners, int* curved, double* curves) {
+    if (!m || !curve_order) return ESDG_E_ARG;
+    const esdg::Mesh& M = m->m;
+    if (M.elem_corners.empty()) {
+        esdg::g_create_error = "mesh_element_curves: the mesh has no corner lists (Cartesian meshes are generated without curves)";
+        return ESDG_E_UNSUPPORTED;
+    }
+    const int mo = M.curve_order, mm = mo > 0 ? mo : 1;
+    *curve_order = mm;
+    if (!corners && !curved && !curves) return ESDG_OK;
+    if (!corners || !curved || !curves) return ESDG_E_ARG;
+    const int K = M.K, stride = M.elem_curves_stride ? M.elem_curves_stride : 2;
+    for (int e = 0; e < K; ++e)
+        for (int k = 0; k < 4; ++k) {
+            const int nd = M.elem_corners[(size_t)e * 4 + k];
+            corners[((size_t)e * 4 + k) * 2 + 0] = M.nodes_x[nd];
+            corners[((size_t)e * 4 + k) * 2 + 1] = M.nodes_y[nd];
+            const int c = M.elem_curved.empty() ? 0 : M.elem_curved[(size_t)e * 4 + k];
+            curved[(size_t)e * 4 + k] = c;
+            for (int j = 0; j <= mm; ++j) {
+                double* o = &curves[(((size_t)e * 4 + k) * (mm + 1) + j) * 2];
+                if (c && j <= mo) {
+                    const double* v = &M.elem_curves[(((size_t)e * 4 + k) * (mo + 1) + j) * stride];
+                    o[0] = v[0]; o[1] = v[1];
+                } else {
+                    o[0] = 0.0; o[1] = 0.0;
+                }
+            }
+        }
+    return ESDG_OK;
+}
+
+int esdg_geometry_device(int N, int K, int curve_order, const double* corners, const int* curved,
+                         const double* curves, double* x, double* y, double* x_xi, double* x_eta, double* y_xi,
+                         double* y_eta, double* J, double* nx_side, double* ny_side, double* scal_side, void* stream) {
+    if (N < 1 || N > 7) { esdg::g_create_error = "geometry_device: N must be in 1..7"; return ESDG_E_UNSUPPORTED; }
+    if (curve_order < 1 || curve_order > esdg::GEO_MAXM) {
+        esdg::g_create_error = "geometry_device: curve order must be in 1.." + std::to_string(esdg::GEO_MAXM);
+        return ESDG_E_UNSUPPORTED;
+    }
+    if (K <= 0 || !corners || !curved || !curves || !x || !y || !x_xi || !x_eta || !y_xi || !y_eta || !J ||
+        !nx_side || !ny_side || !scal_side) {
+        esdg::g_create_error = "geometry_device: K must be positive and every array given";
+        return ESDG_E_ARG;
+    }
+    esdg::Basis B;
+    esdg::build_basis(N, 1, &B);
+    esdg::GeoConst G;
+    std::memset(&G, 0, sizeof G);
+    const int ngl = N + 1;
+    for (int i = 0; i < ngl; ++i) G.xg[i] = B.xGL[i];
+    for (int i = 0; i < ngl * ngl; ++i) G.D0[i] = B.D0[i];
+    esdg::curve_nodes_weights(curve_order, G.xc, G.wb);
+    G.tol = std::pow(10.0, -12);
+    G.m = curve_order;
+    esdg::GeoArgs a{K, corners, curved, curves, x, y, x_xi, x_eta, y_xi, y_eta, J, nx_side, ny_side, scal_side};
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (ngl) {
+#define ESDG_GEO(NG)                                                                                  \
+    case NG: {                                                                                        \
+        using S = esdg::GeoShape<NG>;                                                                 \
+        esdg::k_geometry<NG><<<(K + S::NE - 1) / S::NE, S::THREADS, 0, s>>>(a, G);                    \
+        break;                                                                                        \
+    }
+        ESDG_GEO(2) ESDG_GEO(3) ESDG_GEO(4) ESDG_GEO(5) ESDG_GEO(6) ESDG_GEO(7) ESDG_GEO(8)
+#undef ESDG_GEO
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        esdg::g_create_error = std::string("geometry_device: ") + cudaGetErrorString(e);
+        return ESDG_E_CUDA;
+    }
+    return ESDG_OK;
+}
+
+int esdg_okada_uplift(long long n, const double* x, const double* y, const double* fault, int mercator, int add,
+                      double* out, void* stream) {
+    if (n <= 0 || !x || !y || !fault || !out) {
+        esdg::g_create_error = "okada_uplift: n must be positive and every array given";
+        return ESDG_E_ARG;
+    }
+    // fault: x0, y0, depth, length, width, strike, rake, dip, slip
+    const double x0 = fault[0], y0 = fault[1], depth = fault[2], length = fault[3], width = fault[4];
+    const double strike = fault[5], rake = fault[6], dip = fault[7], slip = fault[8];
+    if (!(width > 0.0) || !(length > 0.0)) {
+        esdg::g_create_error = "okada_uplift: length and width must be positive";
+        return ESDG_E_ARG;
+    }
+    esdg::OkadaConst c;
+    std::memset(&c, 0, sizeof c);
+    const double rad = M_PI / 180.0;
+    const double ang_l = rad * dip, ang_r = rad * rake, ang_t = rad * strike;
+    c.x0 = x0; c.y0 = y0;
+    c.halfl = 0.5 * length; c.width = width;
+    c.hh = depth + width * std::sin(ang_l);
+    c.sn_l = std::sin(ang_l); c.cs_l = std::cos(ang_l);
+    c.sn_t = std::sin(ang_t); c.cs_t = std::cos(ang_t);
+    c.del_x = width * std::cos(ang_l) * std::cos(ang_t);
+    c.del_y = width * std::cos(ang_l) * std::sin(ang_t);
+    c.ds = slip * std::cos(ang_r); c.dd = slip * std::sin(ang_r);
+    c.reach = 1.5 * std::max(length, width);
+    c.R = 6.378e6; c.rad = rad;
+    if (mercator) {
+        const double x0m = x0 * c.R * M_PI / 180.0;
+        const double y0m = c.R * std::asinh(std::tan(y0 / 180.0 * M_PI));
+        c.xlower = x0m - length; c.xupper = x0m + length; c.ylower = y0m - width; c.yupper = y0m + width;
+        c.xo = (c.xlower / c.R) * (180.0 / M_PI);
+        c.yo = std::atan(std::sinh(c.ylower / c.R)) * (180.0 / M_PI);
+        c.yl = c.R * (y0 - c.yo) * rad - c.del_y;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (mercator) esdg::k_okada<true><<<blocks, 256, 0, s>>>((long)n, x, y, c, out, add);
+    else esdg::k_okada<false><<<blocks, 256, 0, s>>>((long)n, x, y, c, out, add);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        esdg::g_create_error = std::string("okada_uplift: ") + cudaGetErrorString(e);
+        return ESDG_E_CUDA;
     }
     return ESDG_OK;
 }

@@ -233,6 +233,11 @@ void Mesh::alloc(int K_, int F_) {
     ElementToEdge.assign((size_t)K * 4, 0);
 }
 
+void curve_nodes_weights(int m, double* xc, double* wb) {
+    for (int k = 0; k <= m; ++k) xc[k] = -std::cos(k * M_PI / m);
+    barycentric_weights(m + 1, xc, wb);
+}
+
 // Curve evaluation on Chebyshev-Gauss-Lobatto samples: src/Mesh.cpp:1861-1987.
 struct Curve {
     int m = 0;                         // polynomial order of the boundary curves

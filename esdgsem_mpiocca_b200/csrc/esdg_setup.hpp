@@ -17,6 +17,9 @@ struct Basis {
 };
 
 void build_basis(int N, int flux_differencing, Basis* B);
+// Boundary-curve sample points -cos(k pi / m), k = 0..m, and their
+// barycentric weights (the interpolation of the element sides).
+void curve_nodes_weights(int m, double* xc, double* wb);
 void lgl_nodes_weights(int N, double* x, double* w);
 void gauss_nodes_weights(int N, double* x, double* w);
 

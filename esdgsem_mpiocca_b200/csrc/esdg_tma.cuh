@@ -125,26 +125,42 @@ constexpr int TMA_VARIANTS = 3;
 __host__ __device__ constexpr int tma_min_blocks(int v) { return v == 1 ? 3 : 2; }
 __host__ __device__ constexpr int tma_stages(int v) { return v == 2 ? 3 : 2; }
 
-template <int NGL, int ST = 2>
-struct TmaShape {
+// One stage buffer of a tile of NE elements: q, gRK (or Qtmp), Jinv, Bx,
+// By, Y_xi, Y_eta, X_xi, X_eta and the element-side face fluxes, each a
+// contiguous section (NE * N2 even: every section starts on 16 bytes).
+template <int NGL, int NE_>
+struct TileLayout {
     static constexpr int N2 = NGL * NGL;
-    // elements per tile: ~256 threads, NE*N2 even (16-byte bulk granularity)
-    static constexpr int NE0 = (256 / N2) > 0 ? (256 / N2) : 1;
-    static constexpr int NE = (N2 % 2 == 1 && NE0 % 2 == 1) ? (NE0 > 1 ? NE0 - 1 : 2) : NE0;
-    static constexpr int THREADS = NE * N2;
-    static constexpr int STAGES = ST;
-    static constexpr int QD = NE * 3 * N2;  // doubles of a q-like section
-    static constexpr int ND = NE * N2;      // doubles of a nodal section
+    static constexpr int NE = NE_;
+    static_assert((NE * N2) % 2 == 0, "16-byte bulk granularity needs NE * N2 even");
+    static constexpr int QD = NE * 3 * N2;    // doubles of a q-like section
+    static constexpr int ND = NE * N2;        // doubles of a nodal section
     static constexpr int FD = NE * 12 * NGL;  // element-side face fluxes of the tile
     static constexpr int STAGE_DOUBLES = 2 * QD + 7 * ND + FD;
-    // shared layout: [STAGES][stage] | su, sv, sh2 [ND each] | sD[N2] | mbar[STAGES]
-    static constexpr size_t SMEM = sizeof(double) * (STAGES * (size_t)STAGE_DOUBLES + 3 * ND + N2) + 16 * STAGES;
 };
 
-// Issues the bulk copies of tile t into stage buffer sb (one thread).
-template <int NGL>
-__device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double* sb, uint64_t* bar) {
-    using S = TmaShape<NGL>;
+// elements per tile of the node-per-thread kernel: ~256 threads, NE*N2 even
+__host__ __device__ constexpr int tma_ne(int n2) {
+    return ((256 / n2) > 0 ? (256 / n2) : 1) % 2 == 1 && n2 % 2 == 1
+               ? ((256 / n2) > 1 ? (256 / n2) - 1 : 2)
+               : ((256 / n2) > 0 ? (256 / n2) : 1);
+}
+
+template <int NGL, int ST = 2>
+struct TmaShape : TileLayout<NGL, tma_ne(NGL * NGL)> {
+    using L = TileLayout<NGL, tma_ne(NGL * NGL)>;
+    static constexpr int THREADS = L::NE * L::N2;
+    static constexpr int STAGES = ST;
+    // shared layout: [STAGES][stage] | su, sv, sh2 [ND each] | sD[N2] | mbar[STAGES]
+    static constexpr size_t SMEM =
+        sizeof(double) * (STAGES * (size_t)L::STAGE_DOUBLES + 3 * L::ND + L::N2) + 16 * STAGES;
+};
+
+// Issues the bulk copies of tile t (NE elements) into stage buffer sb (one
+// thread).
+template <int NGL, int NE>
+__device__ __forceinline__ void tile_issue(const ElemArgs& a, int t, double* sb, uint64_t* bar) {
+    using S = TileLayout<NGL, NE>;
     if (t + 1 == a.skip_tile) return;  // test hook: this tile's copies are never issued
     const int e0 = t * S::NE;
     const int ne = min(S::NE, a.K - e0);
@@ -166,6 +182,11 @@ __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double*
     bulk_g2s(nd + 4 * S::ND, a.Yeta + no, nb, bar);
     bulk_g2s(nd + 5 * S::ND, a.Xxi + no, nb, bar);
     bulk_g2s(nd + 6 * S::ND, a.Xeta + no, nb, bar);
+}
+
+template <int NGL>
+__device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double* sb, uint64_t* bar) {
+    tile_issue<NGL, TmaShape<NGL>::NE>(a, t, sb, bar);
 }
 
 // Persistent flux-differencing volume term + surface lift + RK update

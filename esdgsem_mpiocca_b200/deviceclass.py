@@ -176,6 +176,11 @@ class DeviceClass:
         P, n, margin = _indicator_params(net) if mode >= 2 else (None, 0, 0.0)
         self._ok(self._L.esdg_set_indicator(self.h, mode, P, n, margin))
 
+    def set_indicator_every_stage(self, every_stage: bool):
+        """Learned indicator (modes 2, 3) at every RK stage (default) or once
+        per step, its viscosity and active set kept for the step's stages."""
+        self._ok(self._L.esdg_set_indicator_every_stage(self.h, int(bool(every_stage))))
+
     def indicator_stats(self, reset: bool = False):
         """Counts since the last reset: elements set to zero by the network,
         set to eps0 by the network, decided by the modal sensor, and with

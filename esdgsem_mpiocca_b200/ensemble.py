@@ -102,6 +102,10 @@ class Ensemble:
         P, n, margin = _indicator_params(net) if mode >= 2 else (None, 0, 0.0)
         self._ok(self._L.esdg_ensemble_set_indicator(self.h, mode, P, n, margin))
 
+    def set_indicator_every_stage(self, every_stage: bool):
+        """Learned indicator at every RK stage (default) or once per step."""
+        self._ok(self._L.esdg_ensemble_set_indicator_every_stage(self.h, int(bool(every_stage))))
+
     def indicator_stats(self, reset: bool = False):
         out = (ctypes.c_ulonglong * 4)()
         self._ok(self._L.esdg_ensemble_indicator_stats(self.h, out, int(reset)))

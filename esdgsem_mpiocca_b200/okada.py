@@ -136,3 +136,27 @@ def uplift_cartesian(x_m, y_m, f: Fault):
         u = _dislocation(x1, x2, hh, halfl, f.width, ang_l, ds, dd)
     out[inside] = np.where(np.isfinite(u), u, 0.0)
     return out
+
+
+def uplift_device(x, y, f: Fault, mercator=False, out=None, add=False, stream=None):
+    """The uplift computed on the GPU (esdg_okada_uplift: the same formulas
+    in CUDA) at device points x, y (torch float64 tensors on the current
+    device); returns `out` (a new tensor unless given; with add the uplift
+    is added to it).  mercator selects uplift_mercator's geometry (x, y in
+    Mercator km), else uplift_cartesian's (metres)."""
+    import ctypes
+    import torch
+    from . import lib as _lib
+    x = x.contiguous()
+    y = y.contiguous()
+    if out is None:
+        out = torch.zeros_like(x)
+    fault = np.array([f.x0, f.y0, f.depth, f.length, f.width, f.strike, f.rake, f.dip, f.slip], dtype=np.float64)
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    L = _lib()
+    rc = L.esdg_okada_uplift(int(x.numel()), ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                             fault.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(bool(mercator)),
+                             int(bool(add)), ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s))
+    if rc != 0:
+        raise RuntimeError(f"esdg_okada_uplift failed ({rc}): {L.esdg_last_error(None).decode()}")
+    return out

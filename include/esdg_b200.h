@@ -265,6 +265,16 @@ int esdg_state_pointers(esdg_deviceclass* d, const double** q, const double** b,
  * params/nparams/margin are ignored for modes 0 and 1. */
 int esdg_set_indicator(esdg_deviceclass* d, int mode, const float* params, int nparams, float margin);
 
+/* Schedule of the learned indicator (modes 2 and 3; no counterpart in the
+ * reference): every_stage != 0 (the default) evaluates it at every RK stage,
+ * as the reference evaluates its sensor (src/deviceclass.cpp:1043-1046);
+ * 0 evaluates it once per step, at the step start, and keeps the
+ * viscosity and the active set for the step's stages -- one more
+ * approximation of the learned path, whose deviation from the plain path is
+ * measured like the network's.  Modes 0 and 1 are exact and always run
+ * every stage.  Re-captures the step graph. */
+int esdg_set_indicator_every_stage(esdg_deviceclass* d, int every_stage);
+
 /* Decision counts accumulated over indicator launches: [0] elements the
  * network set to zero, [1] set to eps0, [2] decided by the modal sensor,
  * [3] elements with nonzero viscosity; reset != 0 zeroes them. */
@@ -332,6 +342,8 @@ int esdg_ensemble_set_stream(esdg_ensemble* en, void* cuda_stream);
  * ensemble (re-captures the step graph). */
 int esdg_ensemble_set_indicator(esdg_ensemble* en, int mode, const float* params, int nparams, float margin);
 int esdg_ensemble_indicator_stats(esdg_ensemble* en, unsigned long long* counts4, int reset);
+/* esdg_set_indicator_every_stage for every instance of the ensemble. */
+int esdg_ensemble_set_indicator_every_stage(esdg_ensemble* en, int every_stage);
 /* esdg_set_element_variant / esdg_element_variants for the ensemble's
  * element kernel (no counterpart in the reference). */
 int esdg_ensemble_set_element_variant(esdg_ensemble* en, int variant);
@@ -411,6 +423,39 @@ int esdg_mesh_mapped(int N, double xL, double xR, double yL, double yR, int NX, 
 /* Mesh::ReadMesh (src/Mesh.cpp:698-1503): ISM-V2 reader. */
 int esdg_mesh_read_ism2(int N, const char* path, int read_bottom, int convert_km, esdg_mesh** out);
 int esdg_mesh_write_ism2(const esdg_mesh* m, const char* path);
+
+/* Curvilinear geometry on the device (the set-up's geometry of
+ * src/Mesh.cpp:1000-1081, 1619-1650, 1667-1808 -- boundary-curve transfinite
+ * map, collocation metric terms, Jacobian, side normals -- with every
+ * operation in the host set-up's order, so the same bits).  Inputs are
+ * device arrays: per element its 4 corners (x, y) [K][4][2], per side a
+ * curve flag [K][4] and curve_order + 1 Chebyshev-Gauss-Lobatto samples
+ * (x, y) [K][4][curve_order+1][2] (sides 0 bottom, 1 right, 2 top, 3 left,
+ * as in an ISM-V2 file); outputs x, y, x_xi, x_eta, y_xi, y_eta and J
+ * (not 1/J) [K][N+1][N+1], and the outward unit normal and scale factor of
+ * each side node nx_side, ny_side, scal_side [K][4][N+1].  Runs on `stream`
+ * (NULL: the legacy default stream) without synchronising; allocates
+ * nothing.  esdg_mesh_element_curves exports a host mesh's corners, flags
+ * and samples in that layout (all arrays NULL: only *curve_order). */
+int esdg_mesh_element_curves(const esdg_mesh* m, int* curve_order, double* corners, int* curved, double* curves);
+int esdg_geometry_device(int N, int K, int curve_order, const double* corners, const int* curved,
+                         const double* curves, double* x, double* y, double* x_xi, double* x_eta, double* y_xi,
+                         double* y_eta, double* J, double* nx_side, double* ny_side, double* scal_side, void* stream);
+
+/* Sea-surface uplift of a rectangular fault on the device (Okada 1985
+ * vertical displacement of strike-slip and dip-slip dislocations,
+ * src/okada.cpp:33-249), one value per node: out[i] = uplift, or
+ * out[i] += uplift with add != 0.  fault = {x0, y0, depth, length, width,
+ * strike, rake, dip, slip} (angles in degrees).  mercator != 0: the
+ * reference's geometry -- x, y in Mercator kilometres, (x0, y0) the
+ * epicentre's longitude and latitude, the uplift in kilometres inside the
+ * reference's box; mercator = 0: plane coordinates in metres, (x0, y0) the
+ * fault centroid, the uplift in metres inside a box of half-size
+ * 1.5 max(length, width) (non-finite corner terms give 0).  x, y, out are
+ * device arrays of n values; runs on `stream` without synchronising and
+ * allocates nothing. */
+int esdg_okada_uplift(long long n, const double* x, const double* y, const double* fault, int mercator, int add,
+                      double* out, void* stream);
 
 /* Element and face counts. */
 int esdg_mesh_sizes(const esdg_mesh* m, int* K, int* F);

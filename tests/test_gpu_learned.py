@@ -91,6 +91,38 @@ def test_learned_run_deviation_is_within_tolerance(N, make, steps):
     assert st["net_zero"] + st["net_full"] > 0
 
 
+@pytest.mark.parametrize("N,make,steps", [
+    (3, lambda: problems.tsunami_member(1005, sizes=(64,)), 300),
+])
+def test_learned_once_per_step_deviation_is_within_tolerance(N, make, steps):
+    """The learned indicator evaluated once per step (its viscosity and
+    active set kept for the step's stages) on a tsunami member: the run
+    stays within the same bound of the plain-sensor run, with fewer
+    indicator launches.  (On the N = 4 dam break, whose shocks change the
+    viscosity within a step, this schedule deviates by about 1e-2, outside
+    the bound: it is an option, not the default.)"""
+    prob = make()
+    n2 = (N + 1) ** 2
+    s0 = Solver(prob)
+    s0.run(max_steps=steps)
+    q0 = s0.q()
+    s0.close()
+    launches = {}
+    q = {}
+    for every in (True, False):
+        s2 = Solver(prob, indicator=2, net=IndicatorNet.default(N))
+        s2.dc.set_indicator_every_stage(every)
+        l0 = s2.dc.kernel_launches()
+        s2.run(max_steps=steps)
+        launches[every] = s2.dc.kernel_launches() - l0
+        q[every] = s2.q()
+        s2.close()
+    dev = _rel_l2(q[False], q0, prob.K, n2)
+    assert max(dev) <= TOL_L2, dev
+    assert launches[False] < launches[True]
+    assert np.isfinite(q[False]).all()
+
+
 def _snapshots(prob, every, count):
     """Feature rows, targets and s_eta of the elements of a plain run."""
     import torch
