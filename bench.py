@@ -157,15 +157,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel=""):
-    """DRAM bytes per launch of the element kernel in use, from the
-    committed ncu summary of that kernel."""
-    name = "k_element_rows" if kernel.startswith("k_element_rows") else "k_element"
-    p = os.path.join(ROOT, "profiles", f"{name}_curved_lake_512_N4.md")
-    if not os.path.exists(p):
-        return None
-    with open(p) as f:
-        for line in f:
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of the element-kernel variant in use on this
+    workload, from the committed ncu summary whose title names that exact
+    variant (profiles/<kernel>_curved_lake_512_N4.md); None when no capture
+    of that variant is committed."""
+    import glob
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "k_element*_curved_lake_512_N4.md"))):
+        with open(p) as f:
+            lines = f.read().splitlines()
+        if not lines or not lines[0].startswith("# ") or lines[0][2:].split(" ")[0] != kernel:
+            continue
+        for line in lines:
             if line.startswith("traffic_bytes_per_launch:"):
                 return int(line.split(":")[1].strip())
     return None
@@ -296,6 +299,9 @@ def main():
                     help="ensemble workload: the learned indicator at every RK stage or once per step")
     ap.add_argument("--alone-members", type=int, default=15,
                     help="ensemble workload: members solved one at a time for the plain-path rate")
+    ap.add_argument("--element-variant", type=int, default=-1,
+                    help="curved_lake: fix the element-kernel variant (index into the engine's variant list; "
+                         "-1: the autotuner picks), e.g. to profile one variant")
     args = ap.parse_args()
     if args.workload == "ensemble":
         return ensemble_bench(args)
@@ -318,6 +324,8 @@ def main():
     s = Solver(prob, device_id=local)
     stream = torch.cuda.Stream()
     s.dc.set_stream(stream.cuda_stream)
+    if args.element_variant >= 0:
+        s.dc.set_element_variant(args.element_variant)
     # warm-up: builds the step graph and runs W steps
     s.run(T=1e9, max_steps=args.warmup)
     torch.cuda.synchronize()

@@ -205,7 +205,8 @@ class Engine {
     void release() {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         for (auto& e : pev)
-            if (e) { cudaEventDestroy(e); e = nullptr; }
+            if (e) cudaEventDestroy(e);
+        pev.clear();
         for (auto& b : bufs) cudaFree(b.p);
         bufs.clear();
         bytes = 0;
@@ -1199,10 +1200,13 @@ class Engine {
     // the launching stream around the face and element launches; returns the
     // average duration of each (for roofline reporting).
     int prof_stage_index = -1;
-    cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // per profiled stage: before the face kernel, between the face and the
+    // element kernels, after the element kernel(s); read after the last
+    // step, so the kernels stay queued back to back as in the step graph
+    std::vector<cudaEvent_t> pev;
 
     template <int NGL>
-    void launch_step_profiled(double* face_ms, double* elem_ms) {
+    void launch_step_profiled(cudaEvent_t* pe) {
         if (AV) launch_indicator<NGL>(1);
         k_step_begin<<<(I + 127) / 128, 128, 0, stream>>>(I, st, ngl, AV);
         ++launches;
@@ -1216,9 +1220,10 @@ class Engine {
             const int lam_in_elem = (last && !PP) ? 1 : 0;
             stage_tfrac = stage_time_fraction(s);
             launch_find_dry<NGL>();
-            cudaEventRecord(pev[0], stream);
+            cudaEvent_t* ev = pe + 3 * s;
+            cudaEventRecord(ev[0], stream);
             launch_face<NGL>(AV != 0);
-            cudaEventRecord(pev[1], stream);
+            cudaEventRecord(ev[1], stream);
             if (!AV) {
                 launch_elem_plain<NGL>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem));
             } else {
@@ -1229,18 +1234,12 @@ class Engine {
                 k_element_av2<NGL><<<eb, S::THREADS, 0, stream>>>(elem_args(mode, gA[s], gB[s], gC[s], lam_in_elem));
                 launches += 3;
             }
-            cudaEventRecord(pev[2], stream);
+            cudaEventRecord(ev[2], stream);
             if (PP) {
                 k_pospres<NGL><<<eb, S::THREADS, 0, stream>>>(K, EleSizes, GLw, Jinv, q, elem_inst, st, last ? 1 : 0,
                                                               phys());
                 ++launches;
             }
-            cudaEventSynchronize(pev[2]);
-            float a = 0, b = 0;
-            cudaEventElapsedTime(&a, pev[0], pev[1]);
-            cudaEventElapsedTime(&b, pev[1], pev[2]);
-            *face_ms += a;
-            *elem_ms += b;
         }
         stage_tfrac = 0.0;
         k_step_end<<<(I + 127) / 128, 128, 0, stream>>>(I, st);
@@ -1253,28 +1252,40 @@ class Engine {
         if (r) return r;
         if (gStages <= 0) return fail(ESDG_E_ARG, "profile_steps needs a previous esdg_dg_timeloop call");
         if (AV && indicator) return fail(ESDG_E_UNSUPPORTED, "profile_steps times the reference path (indicator 0)");
-        for (auto& e : pev)
-            if (!e && cudaEventCreate(&e) != cudaSuccess) return fail(ESDG_E_CUDA, "cudaEventCreate");
+        const size_t nev = (size_t)nsteps * gStages * 3;
+        while (pev.size() < nev) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) return fail(ESDG_E_CUDA, "cudaEventCreate");
+            pev.push_back(e);
+        }
         if ((r = poll_state())) return r;
         st_host->done = 0;
         st_host->max_steps = 0;
         st_host->T = 1e300;
         cudaError_t e = cudaMemcpyAsync(st, st_host, sizeof(DevState), cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) return cuda_fail(e, "state upload");
-        double f = 0, el = 0;
         for (int k = 0; k < nsteps; ++k) {
+            cudaEvent_t* pe = pev.data() + (size_t)k * gStages * 3;
             switch (ngl) {
-                case 2: launch_step_profiled<2>(&f, &el); break;
-                case 3: launch_step_profiled<3>(&f, &el); break;
-                case 4: launch_step_profiled<4>(&f, &el); break;
-                case 5: launch_step_profiled<5>(&f, &el); break;
-                case 6: launch_step_profiled<6>(&f, &el); break;
-                case 7: launch_step_profiled<7>(&f, &el); break;
-                case 8: launch_step_profiled<8>(&f, &el); break;
+                case 2: launch_step_profiled<2>(pe); break;
+                case 3: launch_step_profiled<3>(pe); break;
+                case 4: launch_step_profiled<4>(pe); break;
+                case 5: launch_step_profiled<5>(pe); break;
+                case 6: launch_step_profiled<6>(pe); break;
+                case 7: launch_step_profiled<7>(pe); break;
+                case 8: launch_step_profiled<8>(pe); break;
             }
         }
         e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "profile_steps");
+        double f = 0, el = 0;
+        for (size_t k = 0; k < nev; k += 3) {
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, pev[k], pev[k + 1]);
+            cudaEventElapsedTime(&b, pev[k + 1], pev[k + 2]);
+            f += a;
+            el += b;
+        }
         const double nl = (double)nsteps * gStages;
         *face_ms = f / nl;
         *elem_ms = el / nl;
@@ -1579,7 +1590,8 @@ int esdg_set_stream(esdg_deviceclass* d, void* cuda_stream) {
 
 int esdg_profile_steps(esdg_deviceclass* d, int nsteps, double* face_ms, double* elem_ms) {
     ESDG_GUARD(d);
-    if (nsteps <= 0 || !face_ms || !elem_ms) return d->eng.fail(ESDG_E_ARG, "bad profile_steps arguments");
+    if (nsteps <= 0 || nsteps > 1000 || !face_ms || !elem_ms)
+        return d->eng.fail(ESDG_E_ARG, "bad profile_steps arguments");
     return d->eng.profile_steps(nsteps, face_ms, elem_ms);
 }
 

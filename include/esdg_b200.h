@@ -157,7 +157,9 @@ int esdg_advance(esdg_deviceclass* d, int nsteps, double T, double* t_out, int* 
 
 /* Advance nsteps real steps launching kernel by kernel (no graph) with CUDA
  * events recorded on the launching stream around the face-flux and the
- * element launches; returns their average durations in ms per stage. */
+ * element launches; returns their average durations in ms per stage.  All
+ * nsteps steps are queued before the events are read (1 <= nsteps <= 1000),
+ * so the kernels run back to back as in the captured step. */
 int esdg_profile_steps(esdg_deviceclass* d, int nsteps, double* face_ms, double* elem_ms);
 
 /* Element viscosity of the last step (AV only) [K]. */
