@@ -1,0 +1,58 @@
+"""Host logic of bench.py that needs no GPU: the element-kernel name of the
+variant the engine reports, and the DRAM traffic looked up from the
+committed ncu summary of exactly that variant."""
+import os
+
+import bench
+
+
+class _FakeDC:
+    def __init__(self, chosen):
+        self.chosen = chosen
+
+    def element_variants(self):
+        return {"chosen": self.chosen, "count": len(bench.ELEMENT_KERNELS_N4)}
+
+
+def test_element_kernel_name_follows_the_engine_variant():
+    for v, name in enumerate(bench.ELEMENT_KERNELS_N4):
+        assert bench.element_kernel_name(_FakeDC(v)) == name
+    assert bench.element_kernel_name(_FakeDC(-1)) == "k_element<5>"
+
+
+def _summary(path, title, traffic):
+    with open(path, "w") as f:
+        f.write(f"# {title} — curved_lake, N=4, 512x512\n\nsome text\n")
+        if traffic is not None:
+            f.write(f"traffic_bytes_per_launch: {traffic}\n")
+
+
+def test_traffic_comes_from_the_capture_of_the_exact_variant(tmp_path, monkeypatch):
+    prof = tmp_path / "profiles"
+    prof.mkdir()
+    _summary(prof / "k_element_tma_curved_lake_512_N4.md", "k_element_tma<5,3,2>", 1000)
+    _summary(prof / "k_element_pair_curved_lake_512_N4.md", "k_element_pair<5,3>", 2000)
+    _summary(prof / "k_element_rows_curved_lake_512_N4.md", "k_element_rows<5,16,2,2>", None)
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.profiled_traffic("k_element_tma<5,3,2>") == 1000
+    assert bench.profiled_traffic("k_element_pair<5,3>") == 2000
+    # another template instance of a captured kernel, or a summary without
+    # the traffic line: no number
+    assert bench.profiled_traffic("k_element_pair<5,4>") is None
+    assert bench.profiled_traffic("k_element_tma<5,2,2>") is None
+    assert bench.profiled_traffic("k_element_rows<5,16,2,2>") is None
+
+
+def test_committed_traffic_lines_parse():
+    """Every committed element-kernel summary that carries a traffic line
+    names a variant the engine compiles at N = 4."""
+    root = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles")
+    for fn in sorted(os.listdir(root)):
+        if not (fn.startswith("k_element") and fn.endswith("_curved_lake_512_N4.md")):
+            continue
+        with open(os.path.join(root, fn)) as f:
+            text = f.read()
+        title = text.splitlines()[0][2:].split(" ")[0]
+        if "traffic_bytes_per_launch:" in text:
+            assert title in bench.ELEMENT_KERNELS_N4, fn
+            assert bench.profiled_traffic(title) > 0
