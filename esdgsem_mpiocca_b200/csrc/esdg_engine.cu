@@ -1052,7 +1052,6 @@ class Engine {
     }
 
     int capture_step_graph() {
-        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         const long long before = launches;
         cudaGraph_t gr;
         cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
@@ -1060,6 +1059,21 @@ class Engine {
         ESDG_DISPATCH(ngl, launch_step);
         e = cudaStreamEndCapture(stream, &gr);
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        // same launch sequence as the executable graph (the usual case: a
+        // new time loop with the same settings): update its parameters in
+        // place instead of instantiating again
+        if (graph) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(graph, gr, &info) == cudaSuccess) {
+                cudaGraphDestroy(gr);
+                kernels_per_step = (int)(launches - before);
+                launches = before;
+                return 0;
+            }
+            cudaGetLastError();
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
         e = cudaGraphInstantiate(&graph, gr, 0);
         cudaGraphDestroy(gr);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
