@@ -800,7 +800,9 @@ class Engine {
         if (indicator == 2 && FusedShape<NGL>::OK) {
             if constexpr (FusedShape<NGL>::OK) {
                 // features, network and sensor fallback in one pass
-                k_indicator_fused<NGL><<<std::min(ntiles, ind_grid[2]), S::THREADS, 0, stream>>>(ia, ntiles);
+                using FS = FusedShape<NGL>;
+                const int ftiles = (K + FS::NE - 1) / FS::NE;
+                k_indicator_fused<NGL><<<std::min(ftiles, ind_grid[2]), FS::THREADS, 0, stream>>>(ia, ftiles);
                 ++launches;
             }
         } else if (indicator >= 2) {

@@ -413,174 +413,218 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
     }
 }
 
-// The learned indicator in one pass, for degrees whose element is an
-// aligned lane group (n^2 divides 32) and whose tile of NE elements fills
-// whole 16-row MMA tiles: per tile the features of k_ind_features (same
-// arithmetic, same shuffle order) go to a BF16 tile in shared memory, the
-// first NE/16 warps run mlp_warp_forward_regs on it (the arithmetic of
-// k_mlp_forward), and the decision and modal fallback of k_indicator<NGL,
-// true> follow.  The modal transform of an element involves only its own
-// lane group, so it runs per warp (warp barriers) and only in warps that
-// hold an element the network leaves to the sensor.  q and b are read once
-// per stage instead of three passes over q, features and outputs.
+// The learned indicator in one pass at n = 4 (16 nodes per element): four
+// threads per element, thread j of an element holding its nodes j, j + 4,
+// j + 8, j + 12, eight elements per warp.  Every per-element sum is the
+// butterfly of k_ind_features (its offsets 8 and 4 pair nodes inside a
+// thread, 2 and 1 the element's lanes), so the feature rows, the nodal
+// energy and the positivity check are those of k_ind_features bit for bit;
+// the modal transform, its screen and the tail follow k_indicator<NGL, true>
+// entry by entry (entry (k, j) on thread j).  Each warp runs the network on
+// its own eight feature rows (mlp_warp_forward_rows: a 16-row MMA tile with
+// every row present twice, each row's dot products those of k_mlp_forward),
+// and an element's network output arrives in its own lane quad.  Inside the
+// tile loop no warp waits for another; the loads of a tile are issued at its
+// start and the other resident warps cover their latency.
 template <int NGL>
 struct FusedShape {
-    static constexpr int N2 = NGL * NGL, NE = IndShape<NGL>::NE, THREADS = IndShape<NGL>::THREADS;
+    static constexpr int N2 = NGL * NGL;
+    static constexpr int TPE = 4;                   // threads per element
+    static constexpr int NPT = N2 / TPE;            // nodes per thread
+    static constexpr int EPW = 32 / TPE;            // elements per warp
+    static constexpr int THREADS = 256;
+    static constexpr int NE = EPW * (THREADS / 32);  // elements per tile
     static constexpr int KP = mlp_kp(NGL);
-    static constexpr int MT = NE / 16;  // MMA row tiles per element tile
-    static constexpr bool OK = (32 % N2) == 0 && NE % 16 == 0 && MT <= THREADS / 32 && NGL >= 4 && NGL <= 6;
+    static constexpr int XS = KP + 8;               // feature / W1 row stride (bf16), bank-conflict free
+    static constexpr int W2S = MLP_H + 8;           // W2 row stride (bf16)
+    static constexpr int ES = N2 + 1;               // element stride of the modal arrays (doubles)
+    static constexpr bool OK = NGL == 4;            // NPT = 4: the butterfly's two inner levels
 };
+
+// Sum of the element's 16 node values x[k] (node j + 4k on thread j) in the
+// order of a 16-lane xor butterfly with offsets 8, 4, 2, 1.
+__device__ __forceinline__ double quad_sum16(const double (&x)[4]) {
+    double s = (x[0] + x[2]) + (x[1] + x[3]);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    return s;
+}
+__device__ __forceinline__ float quad_sum16f(const float (&x)[4]) {
+    float s = (x[0] + x[2]) + (x[1] + x[3]);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    return s;
+}
 
 template <int NGL>
 __global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused(IndArgs a, int ntiles) {
     using S = FusedShape<NGL>;
-    constexpr int N2 = S::N2, NE = S::NE, KP = S::KP;
-    static_assert(S::OK, "fused indicator: element = aligned lane group, whole 16-row tiles");
+    constexpr int N2 = S::N2, NE = S::NE, KP = S::KP, XS = S::XS, W2S = S::W2S, ES = S::ES;
+    constexpr int NPT = S::NPT, TPE = S::TPE, EPW = S::EPW;
+    static_assert(S::OK, "fused indicator: n = 4");
     if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
-    __shared__ __align__(16) __nv_bfloat16 sW1[MLP_H * KP];
-    __shared__ __align__(16) __nv_bfloat16 sW2[MLP_H * MLP_H];
-    __shared__ __align__(16) __nv_bfloat16 sX[NE * KP];
-    __shared__ float sy[NE], sseta[NE];
+    __shared__ __align__(16) __nv_bfloat16 sW1[MLP_H * XS];
+    __shared__ __align__(16) __nv_bfloat16 sW2[MLP_H * W2S];
+    __shared__ __align__(16) __nv_bfloat16 sX[NE * XS];
+    __shared__ __align__(16) float sP32[3 * MLP_H + 4];  // b1, b2, w3, b3
     __shared__ double sV[N2];
-    __shared__ double seta[NE * N2], sM[NE * N2], sW[NE * N2];
+    __shared__ double seta[NE * ES], sM[NE * ES], sW[NE * ES];
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int el = tid / N2, nd = tid % N2;
-    const int s = el * N2 + nd;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int el = tid / TPE, j = tid % TPE;
     if (tid < N2) sV[tid] = a.Vinv[tid];
-    mlp_stage_weights(KP, a.Pb, a.L, sW1, sW2);
-    MlpLaneParams R{};
-    if (warp < S::MT) R = mlp_lane_params(a.P, a.L);
-    __syncthreads();
-    struct Ld {
-        double h, b, hu, hv;
-        int ins;
-        int4 nb;
-    };
-    auto fetch = [&](int t) {
-        Ld L{1.0, 0.0, 0.0, 0.0, -1, make_int4(-1, -1, -1, -1)};
-        const int e = t * NE + el;
-        if (e < a.K) {
-            const long qid = (long)e * 3 * N2 + nd;
-            L.h = a.q[qid];
-            L.b = a.B[(long)e * N2 + nd];
-            L.hu = a.q[qid + N2];
-            L.hv = a.q[qid + 2 * N2];
-            L.ins = inst_of(a.elem_inst, e);
-            if (nd == 0 && a.act) L.nb = a.nbr[e];
-        }
-        return L;
-    };
+    for (int i = tid; i < MLP_H * KP; i += blockDim.x) sW1[(i / KP) * XS + i % KP] = a.Pb[a.L.w1 + i];
+    for (int i = tid; i < MLP_H * MLP_H; i += blockDim.x) sW2[(i / MLP_H) * W2S + i % MLP_H] = a.Pb[a.L.w2 + i];
+    for (int i = tid; i < MLP_H; i += blockDim.x) {
+        sP32[i] = a.P[a.L.b1 + i];
+        sP32[MLP_H + i] = a.P[a.L.b2 + i];
+        sP32[2 * MLP_H + i] = a.P[a.L.w3 + i];
+    }
+    if (tid == 0) sP32[3 * MLP_H] = a.P[a.L.b3];
+    __syncthreads();  // the only block barrier: V and the network staged
+    double* se = seta + el * ES;
+    double* sm = sM + el * ES;
+    double* sw = sW + el * ES;
+    __nv_bfloat16* xr = sX + el * XS;
     unsigned long long cnt[4] = {0, 0, 0, 0};
-    int t = blockIdx.x;
-    Ld nxt = (t < ntiles) ? fetch(t) : Ld{1.0, 0.0, 0.0, 0.0, -1, make_int4(-1, -1, -1, -1)};
-    for (; t < ntiles; t += gridDim.x) {
-        const Ld cur = nxt;
-        if (t + gridDim.x < ntiles) nxt = fetch(t + gridDim.x);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int e = t * NE + el;
-        const bool live = e < a.K && !a.st[cur.ins].done;
-        // ---- features (k_ind_features) ----
-        const double v3[3] = {cur.b + cur.h, cur.hu, cur.hv};
-        seta[s] = v3[0];
-        double mh = cur.h, e2 = v3[0] * v3[0];
-        bool fin = isfinite(cur.h) && isfinite(cur.hu) && isfinite(cur.hv);
-        double m3[3] = {v3[0], v3[1], v3[2]};
+        const bool inb = e < a.K;
+        // node j + 4k of the element: h, eta = b + h, hu, hv (idle elements
+        // take h = 1, b = 0, hu = hv = 0 so that every value stays finite)
+        double h[NPT], v0[NPT], v1[NPT], v2[NPT];
+        int ins = 0;
+        int4 nb = make_int4(-1, -1, -1, -1);
+        if (inb) {
+            const double* qe = a.q + (long)e * 3 * N2;
+            const double* be = a.B + (long)e * N2;
 #pragma unroll
-        for (int off = N2 / 2; off > 0; off >>= 1) {
+            for (int k = 0; k < NPT; ++k) {
+                const int p = j + TPE * k;
+                h[k] = qe[p];
+                v1[k] = qe[p + N2];
+                v2[k] = qe[p + 2 * N2];
+                v0[k] = be[p] + h[k];
+            }
+            ins = inst_of(a.elem_inst, e);
+            if (j == 0 && a.act) nb = a.nbr[e];
+        } else {
 #pragma unroll
-            for (int f = 0; f < 3; ++f) m3[f] += __shfl_xor_sync(0xffffffffu, m3[f], off);
-            mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
-            e2 += __shfl_xor_sync(0xffffffffu, e2, off);
-            fin = __shfl_xor_sync(0xffffffffu, (int)fin, off) && fin;
+            for (int k = 0; k < NPT; ++k) {
+                h[k] = 1.0; v1[k] = 0.0; v2[k] = 0.0; v0[k] = 0.0 + 1.0;
+            }
         }
-        float dv[3], d3f[3];
+        const bool live = inb && !a.st[ins].done;
+        // ---- features (k_ind_features) ----
+        double e2k[NPT];
+        bool fin = true;
+        double mh = fmin(fmin(h[0], h[2]), fmin(h[1], h[3]));
+#pragma unroll
+        for (int k = 0; k < NPT; ++k) {
+            se[j + TPE * k] = v0[k];
+            e2k[k] = v0[k] * v0[k];
+            fin = fin && isfinite(h[k]) && isfinite(v1[k]) && isfinite(v2[k]);
+        }
+        double m3[3] = {quad_sum16(v0), quad_sum16(v1), quad_sum16(v2)};
+        const double e2 = quad_sum16(e2k);
+        mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, 2));
+        mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, 1));
+        fin = __shfl_xor_sync(0xffffffffu, (int)fin, 2) && fin;
+        fin = __shfl_xor_sync(0xffffffffu, (int)fin, 1) && fin;
+        float dv[3][NPT], rmsf[3];
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
             m3[f] /= N2;
-            dv[f] = (float)(v3[f] - m3[f]);
-            d3f[f] = dv[f] * dv[f];
-        }
+            float d3[NPT];
 #pragma unroll
-        for (int off = N2 / 2; off > 0; off >>= 1)
-#pragma unroll
-            for (int f = 0; f < 3; ++f) d3f[f] += __shfl_xor_sync(0xffffffffu, d3f[f], off);
-        __nv_bfloat16* xr = sX + el * KP;
-        float rmsf[3];
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-            rmsf[f] = sqrtf(d3f[f] * (1.0f / N2));
+            for (int k = 0; k < NPT; ++k) {
+                const double v = f == 0 ? v0[k] : (f == 1 ? v1[k] : v2[k]);
+                dv[f][k] = (float)(v - m3[f]);
+                d3[k] = dv[f][k] * dv[f][k];
+            }
+            rmsf[f] = sqrtf(quad_sum16f(d3) * (1.0f / N2));
             const float mf = fabsf((float)m3[f]);
             const float inv = (rmsf[f] > (float)MLP_REL_FLAT * mf && rmsf[f] > 0.0f) ? 1.0f / rmsf[f] : 0.0f;
-            xr[f * N2 + nd] = __float2bfloat16(dv[f] * inv);
+#pragma unroll
+            for (int k = 0; k < NPT; ++k) xr[f * N2 + j + TPE * k] = __float2bfloat16(dv[f][k] * inv);
         }
-        if (nd < 3) {  // lanes 0, 1, 2 of the group: the scale feature of their field
-            const float r = nd == 0 ? rmsf[0] : (nd == 1 ? rmsf[1] : rmsf[2]);
-            const float m = (float)(nd == 0 ? m3[0] : (nd == 1 ? m3[1] : m3[2]));
+        float sf = 0.0f;
+        if (j < 3) {  // threads 0, 1, 2 of the element: the scale feature of their field
+            const float r = j == 0 ? rmsf[0] : (j == 1 ? rmsf[1] : rmsf[2]);
+            const float m = (float)(j == 0 ? m3[0] : (j == 1 ? m3[1] : m3[2]));
             const float tot = m * m + r * r;
-            const float sf = (tot > 0.0f && r > 0.0f) ? fmaxf(log10f(r * r / tot), (float)MLP_S_MIN) : (float)MLP_S_MIN;
-            xr[3 * N2 + nd] = __float2bfloat16(0.25f * sf);
-            if (nd == 0) sseta[el] = sf;
+            sf = (tot > 0.0f && r > 0.0f) ? fmaxf(log10f(r * r / tot), (float)MLP_S_MIN) : (float)MLP_S_MIN;
+            xr[3 * N2 + j] = __float2bfloat16(0.25f * sf);
         }
-        for (int c = 3 * N2 + 3 + nd; c < KP; c += N2) xr[c] = __float2bfloat16(0.0f);
+        for (int c = 3 * N2 + 3 + j; c < KP; c += TPE) xr[c] = __float2bfloat16(0.0f);
+        const float s_eta = __shfl_sync(0xffffffffu, sf, lane & ~(TPE - 1));
         const int ok = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
-        __syncthreads();  // feature tile complete
-        // ---- network (k_mlp_forward) ----
-        if (warp < S::MT) {
-            float ylo, yhi;
-            mlp_warp_forward_regs<KP>(sX + warp * 16 * KP, sW1, sW2, R, ylo, yhi);
-            if ((lane & 3) == 0) {
-                sy[warp * 16 + (lane >> 2)] = ylo;
-                sy[warp * 16 + (lane >> 2) + 8] = yhi;
-            }
-        }
-        __syncthreads();  // outputs complete; the feature tile may be rewritten after this
-        // ---- decision and modal fallback (k_indicator<NGL, true>), per lane group ----
+        __syncwarp();  // the warp's feature rows complete
+        // ---- network (k_mlp_forward) on the warp's eight rows ----
+        const float y = mlp_warp_forward_rows<KP, EPW, XS, XS, W2S>(sX + warp * EPW * XS, sW1, sW2, sP32);
+        // ---- decision and modal fallback (k_indicator<NGL, true>) ----
         int nm = 1, vd = 0;
         if (live) {
-            const double sig = (double)sy[el] + (double)sseta[el];
+            const double sig = (double)y + (double)s_eta;
             nm = learned_needs_modal(a, sig, e2, ok);
             vd = (nm == 0 && a.emax * e2 >= a.c.ZeroTOL && sig > a.c.sigmaMax + a.margin) ? 1 : 0;
         }
         bool clear = false;
         if (__any_sync(0xffffffffu, live && nm)) {
-            const int i = nd / NGL, j = nd % NGL;  // entry (i, j) of M1 and w
-            sM[s] = sensor_m1<NGL>(sV, seta + el * N2, i, j);
-            __syncwarp();
-            sW[s] = sensor_w<NGL>(sV, sM + el * N2, i, j);
-            __syncwarp();
-            const double w = sW[s], w2 = w * w;
-            constexpr int N = NGL - 1;
-            double z1 = ((i == N) || (j == N)) ? w2 : 0.0;
-            double z2 = (((i == N - 1) && (j <= N - 1)) || ((j == N - 1) && (i <= N - 1))) ? w2 : 0.0;
-            double n1 = w2;
-            double n2 = (i < N && j < N) ? w2 : 0.0;
+            // entries (k, j), k = 0..NGL-1, of M1 = V m^T and w = M1 V^T
+            // (sensor_m1, sensor_w: the same products and sums)
+            double mrow[NGL];
 #pragma unroll
-            for (int off = N2 / 2; off > 0; off >>= 1) {
-                z1 += __shfl_xor_sync(0xffffffffu, z1, off);
-                z2 += __shfl_xor_sync(0xffffffffu, z2, off);
-                n1 += __shfl_xor_sync(0xffffffffu, n1, off);
-                n2 += __shfl_xor_sync(0xffffffffu, n2, off);
+            for (int l = 0; l < NGL; ++l) mrow[l] = se[j * NGL + l];
+#pragma unroll
+            for (int k = 0; k < NGL; ++k) {
+                double acc = 0.0;
+#pragma unroll
+                for (int l = 0; l < NGL; ++l) acc += sV[k * NGL + l] * mrow[l];
+                sm[k * NGL + j] = acc;
             }
+            __syncwarp();
+            double w[NGL];
+#pragma unroll
+            for (int k = 0; k < NGL; ++k) {
+                double acc = 0.0;
+#pragma unroll
+                for (int l = 0; l < NGL; ++l) acc += sm[k * NGL + l] * sV[j * NGL + l];
+                w[k] = acc;
+                sw[k * NGL + j] = acc;
+            }
+            __syncwarp();
+            constexpr int N = NGL - 1;
+            double z1[NPT], z2[NPT], n1[NPT], n2[NPT];
+#pragma unroll
+            for (int k = 0; k < NPT; ++k) {  // entry (i, jj) = (k, j)
+                const double w2 = w[k] * w[k];
+                z1[k] = ((k == N) || (j == N)) ? w2 : 0.0;
+                z2[k] = (((k == N - 1) && (j <= N - 1)) || ((j == N - 1) && (k <= N - 1))) ? w2 : 0.0;
+                n1[k] = w2;
+                n2[k] = (k < N && j < N) ? w2 : 0.0;
+            }
+            const double Z1 = quad_sum16(z1), Z2 = quad_sum16(z2), N1 = quad_sum16(n1), N2s = quad_sum16(n2);
             const double thr = a.c.sensor_skip * (1.0 - 1e-6);
-            clear = n1 > a.c.ZeroTOL * (1.0 + 1e-6) && z1 < thr * n1 && z2 < thr * n2;
-            clear = clear || (n1 < a.c.ZeroTOL * (1.0 - 1e-6));
+            clear = N1 > a.c.ZeroTOL * (1.0 + 1e-6) && Z1 < thr * N1 && Z2 < thr * N2s;
+            clear = clear || (N1 < a.c.ZeroTOL * (1.0 - 1e-6));
         }
-        if (live && nd == 0) {
+        if (live && j == 0) {
             double v = 0.0;
             int kind = 2;  // 0 net zero, 1 net eps0, 2 modal
             if (nm) {
-                v = clear ? 0.0 : sensor_tail<NGL>(a.c, sW + el * N2);
+                v = clear ? 0.0 : sensor_tail<NGL>(a.c, sw);
             } else {
                 kind = vd;
                 v = kind ? a.c.eps0 : 0.0;
             }
             a.VP[e] = v;
-            if (a.stage0 && v > 0.0) atomicMax(&a.st[cur.ins].visc_key, dbl_key(v));
-            if (a.act && !(v <= 0.0)) mark_active(a.act, e, cur.nb);
+            if (a.stage0 && v > 0.0) atomicMax(&a.st[ins].visc_key, dbl_key(v));
+            if (a.act && !(v <= 0.0)) mark_active(a.act, e, nb);
             cnt[kind] += 1;
             if (!(v <= 0.0)) cnt[3] += 1;
         }
-        __syncwarp();  // the group's shared rows are rewritten next tile
+        __syncwarp();  // the warp's shared rows are rewritten next tile
     }
     if (a.stats) {
 #pragma unroll

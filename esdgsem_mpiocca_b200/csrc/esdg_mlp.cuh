@@ -345,6 +345,74 @@ __device__ __forceinline__ void mlp_warp_forward_regs(const __nv_bfloat16* X, co
     y_hi = hi + R.b3;
 }
 
+// The same forward pass for a warp that holds only R rows (R divides 8):
+// row r of the 16-row MMA tile is row r % R of X, so a0 = a1 and a2 = a3,
+// and every row's dot products are those mlp_warp_forward_regs forms for it
+// in a full tile (the same operands, MMAs and FP32 additions, in the same
+// order).  Biases and w3 come from shared memory (P32: b1, b2, w3 [32 each],
+// b3), so a warp keeps no network parameters in registers between tiles.
+// Lane 4 r holds y of row r (r < R).
+// Row strides (bf16 elements): XS of X, W1S of W1 [32][W1S], W2S of W2
+// [32][W2S]; strides of KP + 8 and 40 keep the fragment loads of a warp free
+// of shared-memory bank conflicts.
+template <int KP, int R, int XS = KP, int W1S = KP, int W2S = MLP_H>
+__device__ __forceinline__ float mlp_warp_forward_rows(const __nv_bfloat16* X, const __nv_bfloat16* W1,
+                                                       const __nv_bfloat16* W2, const float* P32) {
+    static_assert(8 % R == 0, "rows per warp divide 8");
+    static_assert(XS % 8 == 0 && W1S % 8 == 0 && W2S % 8 == 0, "16-byte rows");
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int row = g % R;
+    const unsigned* Xu = reinterpret_cast<const unsigned*>(X);
+    const unsigned* W1u = reinterpret_cast<const unsigned*>(W1);
+    const unsigned* W2u = reinterpret_cast<const unsigned*>(W2);
+    const float2* b1 = reinterpret_cast<const float2*>(P32);
+    const float2* b2 = reinterpret_cast<const float2*>(P32 + MLP_H);
+    const float2* w3 = reinterpret_cast<const float2*>(P32 + 2 * MLP_H);
+    float acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float2 b = b1[4 * j + t];
+        acc[j][0] = b.x; acc[j][1] = b.y; acc[j][2] = b.x; acc[j][3] = b.y;
+    }
+#pragma unroll
+    for (int kb = 0; kb < KP / 16; ++kb) {
+        const int c = kb * 8 + t;
+        const unsigned a0 = Xu[row * (XS / 2) + c], a2 = Xu[row * (XS / 2) + c + 4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = 8 * j + g;
+            mlp_mma16816(acc[j], a0, a0, a2, a2, W1u[n * (W1S / 2) + c], W1u[n * (W1S / 2) + c + 4]);
+        }
+    }
+    float acc2[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float2 b = b2[4 * j + t];
+        acc2[j][0] = b.x; acc2[j][1] = b.y; acc2[j][2] = b.x; acc2[j][3] = b.y;
+    }
+#pragma unroll
+    for (int kb = 0; kb < 2; ++kb) {
+        const int j0 = 2 * kb, j1 = 2 * kb + 1;
+        const unsigned a0 = mlp_pack_bf16(fmaxf(acc[j0][0], 0.f), fmaxf(acc[j0][1], 0.f));
+        const unsigned a2 = mlp_pack_bf16(fmaxf(acc[j1][0], 0.f), fmaxf(acc[j1][1], 0.f));
+        const int c = kb * 8 + t;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = 8 * j + g;
+            mlp_mma16816(acc2[j], a0, a0, a2, a2, W2u[n * (W2S / 2) + c], W2u[n * (W2S / 2) + c + 4]);
+        }
+    }
+    float lo = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float2 w = w3[4 * j + t];
+        lo += fmaxf(acc2[j][0], 0.f) * w.x + fmaxf(acc2[j][1], 0.f) * w.y;
+    }
+    lo += __shfl_xor_sync(0xffffffffu, lo, 1);
+    lo += __shfl_xor_sync(0xffffffffu, lo, 2);
+    return lo + P32[3 * MLP_H];
+}
+
 // Shared-memory carve-up of the MLP kernels (bytes): the BF16 weights once
 // per block, then per warp: X tile, A1 (bf16), Z (float), dZ2 and dZ1
 // (bf16), scratch (float), y.
