@@ -75,6 +75,23 @@ def sum_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
     return float(t.item())
 
 
+def job_rate(work: float, ms: float, dist=None, device: str = "cuda") -> float:
+    """Whole-job rate of weakly scaled ranks: the work of all ranks over the
+    slowest rank's time (ms)."""
+    return sum_over_ranks(work, dist, device) / (max_over_ranks(ms, dist, device) / 1e3)
+
+
+def ensemble_summary(dofs: float, ms: float, steps: int, alone_dofs: float, alone_ms: float, dev: float,
+                     dist=None, device: str = "cuda"):
+    """The ensemble line's rank aggregation: the batched rate of all ranks'
+    members over the slowest rank's timed steps, the one-at-a-time rate as
+    the sum of the ranks' own rates (each GPU solves its sample alone), and
+    the largest deviation of any rank."""
+    rate = job_rate(dofs * STAGES * steps, ms, dist, device)
+    alone = sum_over_ranks(alone_dofs * STAGES * steps / (alone_ms / 1e3), dist, device)
+    return rate, alone, max_over_ranks(dev, dist, device)
+
+
 def member_seeds(rank: int, members: int) -> list:
     """Ensemble members of one rank: disjoint seed ranges, no exchange."""
     return list(range(rank * members, (rank + 1) * members))
@@ -348,8 +365,7 @@ def main():
     launches = s.dc.kernel_launches() - launches0
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, dist)
-    dof_stages = sum_over_ranks(prob.dofs() * STAGES * args.steps, dist)
-    value = dof_stages / (ms_max / 1e3)
+    value = job_rate(prob.dofs() * STAGES * args.steps, ms, dist)
 
     # ---- dominant kernel duration, timed live on the engine's stream ----
     kern = time_element_kernel(s, stream, prob)
@@ -572,9 +588,7 @@ def ensemble_measure(members, steps, warm, alone_members, local, dist, ws, rank,
         agree += int(((v0 > 0) == (v2 > 0)).sum())
         nflag += int(v0.size)
         s.close()
-    alone = adofs * STAGES * steps / (ams / 1e3)  # per GPU (one request at a time per GPU)
-    alone = sum_over_ranks(alone, dist)
-    dev = max_over_ranks(dev, dist)
+    _, alone, dev = ensemble_summary(dofs, learned["ms"], steps, adofs, ams, dev, dist)
     stt = learned["stats"]
     decided = stt["net_zero"] + stt["net_full"]
     evals = decided + stt["modal"]
