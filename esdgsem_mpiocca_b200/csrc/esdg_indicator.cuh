@@ -413,24 +413,28 @@ __global__ void __launch_bounds__(IndShape<NGL>::THREADS, 3) k_indicator(IndArgs
     }
 }
 
-// The learned indicator in one pass at n = 4 (16 nodes per element): four
-// threads per element, thread j of an element holding its nodes j, j + 4,
-// j + 8, j + 12, eight elements per warp.  Every per-element sum is the
-// butterfly of k_ind_features (its offsets 8 and 4 pair nodes inside a
-// thread, 2 and 1 the element's lanes), so the feature rows, the nodal
-// energy and the positivity check are those of k_ind_features bit for bit;
-// the modal transform, its screen and the tail follow k_indicator<NGL, true>
-// entry by entry (entry (k, j) on thread j).  Each warp runs the network on
-// its own eight feature rows (mlp_warp_forward_rows: a 16-row MMA tile with
-// every row present twice, each row's dot products those of k_mlp_forward),
-// and an element's network output arrives in its own lane quad.  Inside the
-// tile loop no warp waits for another; the loads of a tile are issued at its
-// start and the other resident warps cover their latency.
+// The learned indicator in one pass at n = 4 and n = 5.  The feature pass
+// it replaces reduces each element over a butterfly of W lanes (W = 16 at
+// n = 4: k_ind_features, one lane per node; W = 32 at n = 5:
+// k_ind_features_warp, one warp per element, lanes past the 25th node
+// contributing zeros).  Here W / 4 threads hold an element, thread j its
+// butterfly slots j, j + W/4, j + W/2, j + 3W/4 (node = slot where the slot
+// is a node): the butterfly's two widest levels pair slots inside a thread,
+// the rest the element's lanes, so every per-element sum -- means, nodal
+// energy, deviations -- and the positivity check are those of the feature
+// pass bit for bit.  The modal transform, its screen (n = 4, as in
+// k_indicator<4, true>) and the tail follow k_indicator<NGL, true> entry by
+// entry.  Each warp runs the network on its own 32 / (W/4) feature rows
+// (mlp_warp_forward_rows: a 16-row MMA tile with every row repeated, each
+// row's dot products those of k_mlp_forward).  Inside the tile loop no warp
+// waits for another; a tile's loads are issued at its start and the other
+// resident warps cover their latency.
 template <int NGL>
 struct FusedShape {
     static constexpr int N2 = NGL * NGL;
-    static constexpr int TPE = 4;                   // threads per element
-    static constexpr int NPT = N2 / TPE;            // nodes per thread
+    static constexpr int W = N2 <= 16 ? 16 : 32;    // butterfly width of the feature pass
+    static constexpr int SLOTS = 4;                 // butterfly slots per thread
+    static constexpr int TPE = W / SLOTS;           // threads per element
     static constexpr int EPW = 32 / TPE;            // elements per warp
     static constexpr int THREADS = 256;
     static constexpr int NE = EPW * (THREADS / 32);  // elements per tile
@@ -438,21 +442,17 @@ struct FusedShape {
     static constexpr int XS = KP + 8;               // feature / W1 row stride (bf16), bank-conflict free
     static constexpr int W2S = MLP_H + 8;           // W2 row stride (bf16)
     static constexpr int ES = N2 + 1;               // element stride of the modal arrays (doubles)
-    static constexpr bool OK = NGL == 4;            // NPT = 4: the butterfly's two inner levels
+    static constexpr bool SCREEN = (32 % N2) == 0;  // k_indicator's any-order screen (aligned lane groups)
+    static constexpr bool OK = NGL == 4 || NGL == 5;
 };
 
-// Sum of the element's 16 node values x[k] (node j + 4k on thread j) in the
-// order of a 16-lane xor butterfly with offsets 8, 4, 2, 1.
-__device__ __forceinline__ double quad_sum16(const double (&x)[4]) {
-    double s = (x[0] + x[2]) + (x[1] + x[3]);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    return s;
-}
-__device__ __forceinline__ float quad_sum16f(const float (&x)[4]) {
-    float s = (x[0] + x[2]) + (x[1] + x[3]);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
+// Sum over an element's W butterfly slots x[k] (slot j + k W/4 on thread j
+// of the element's W/4 lanes), in the order of a W-lane xor butterfly.
+template <int TPE, typename T>
+__device__ __forceinline__ T slot_sum(const T (&x)[4]) {
+    T s = (x[0] + x[2]) + (x[1] + x[3]);
+#pragma unroll
+    for (int off = TPE / 2; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     return s;
 }
 
@@ -460,8 +460,8 @@ template <int NGL>
 __global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused(IndArgs a, int ntiles) {
     using S = FusedShape<NGL>;
     constexpr int N2 = S::N2, NE = S::NE, KP = S::KP, XS = S::XS, W2S = S::W2S, ES = S::ES;
-    constexpr int NPT = S::NPT, TPE = S::TPE, EPW = S::EPW;
-    static_assert(S::OK, "fused indicator: n = 4");
+    constexpr int TPE = S::TPE, EPW = S::EPW;
+    static_assert(S::OK, "fused indicator: n = 4 or 5");
     if (a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     __shared__ __align__(16) __nv_bfloat16 sW1[MLP_H * XS];
     __shared__ __align__(16) __nv_bfloat16 sW2[MLP_H * W2S];
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int el = tid / TPE, j = tid % TPE;
-    if (tid < N2) sV[tid] = a.Vinv[tid];
+    for (int i = tid; i < N2; i += blockDim.x) sV[i] = a.Vinv[i];
     for (int i = tid; i < MLP_H * KP; i += blockDim.x) sW1[(i / KP) * XS + i % KP] = a.Pb[a.L.w1 + i];
     for (int i = tid; i < MLP_H * MLP_H; i += blockDim.x) sW2[(i / MLP_H) * W2S + i % MLP_H] = a.Pb[a.L.w2 + i];
     for (int i = tid; i < MLP_H; i += blockDim.x) {
@@ -490,63 +490,84 @@ __global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int e = t * NE + el;
         const bool inb = e < a.K;
-        // node j + 4k of the element: h, eta = b + h, hu, hv (idle elements
-        // take h = 1, b = 0, hu = hv = 0 so that every value stays finite)
-        double h[NPT], v0[NPT], v1[NPT], v2[NPT];
+        // slot k = node j + TPE k: h, eta = b + h, hu, hv.  Slots past the
+        // last node hold zeros and mh's start value (as the feature pass's
+        // idle lanes); idle elements take h = 1, b = 0, hu = hv = 0.
+        double h[4], v0[4], v1[4], v2[4];
+        bool val[4];
         int ins = 0;
         int4 nb = make_int4(-1, -1, -1, -1);
-        if (inb) {
-            const double* qe = a.q + (long)e * 3 * N2;
-            const double* be = a.B + (long)e * N2;
+        const double* qe = a.q + (long)(inb ? e : 0) * 3 * N2;
+        const double* be = a.B + (long)(inb ? e : 0) * N2;
 #pragma unroll
-            for (int k = 0; k < NPT; ++k) {
-                const int p = j + TPE * k;
+        for (int k = 0; k < 4; ++k) {
+            const int p = j + TPE * k;
+            val[k] = p < N2;
+            h[k] = 1.0; v0[k] = 0.0; v1[k] = 0.0; v2[k] = 0.0;
+            if (inb && val[k]) {
                 h[k] = qe[p];
                 v1[k] = qe[p + N2];
                 v2[k] = qe[p + 2 * N2];
                 v0[k] = be[p] + h[k];
+            } else if (val[k]) {
+                v0[k] = 0.0 + 1.0;
             }
+        }
+        if (inb) {
             ins = inst_of(a.elem_inst, e);
             if (j == 0 && a.act) nb = a.nbr[e];
-        } else {
-#pragma unroll
-            for (int k = 0; k < NPT; ++k) {
-                h[k] = 1.0; v1[k] = 0.0; v2[k] = 0.0; v0[k] = 0.0 + 1.0;
-            }
         }
         const bool live = inb && !a.st[ins].done;
-        // ---- features (k_ind_features) ----
-        double e2k[NPT];
+        // ---- features (the feature pass) ----
+        double e2k[4], mhk[4];
         bool fin = true;
-        double mh = fmin(fmin(h[0], h[2]), fmin(h[1], h[3]));
 #pragma unroll
-        for (int k = 0; k < NPT; ++k) {
-            se[j + TPE * k] = v0[k];
-            e2k[k] = v0[k] * v0[k];
-            fin = fin && isfinite(h[k]) && isfinite(v1[k]) && isfinite(v2[k]);
+        for (int k = 0; k < 4; ++k) {
+            const int p = j + TPE * k;
+            if (val[k]) se[p] = v0[k];
+            e2k[k] = val[k] ? v0[k] * v0[k] : 0.0;
+            mhk[k] = val[k] ? h[k] : 1e300;
+            fin = fin && (!val[k] || (isfinite(h[k]) && isfinite(v1[k]) && isfinite(v2[k])));
         }
-        double m3[3] = {quad_sum16(v0), quad_sum16(v1), quad_sum16(v2)};
-        const double e2 = quad_sum16(e2k);
-        mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, 2));
-        mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, 1));
-        fin = __shfl_xor_sync(0xffffffffu, (int)fin, 2) && fin;
-        fin = __shfl_xor_sync(0xffffffffu, (int)fin, 1) && fin;
-        float dv[3][NPT], rmsf[3];
+        // the warp-per-element pass (n = 5) starts each lane's sum at 0.0
+        // (0.0 + v turns -0.0 into +0.0); the lane-per-node pass sums v
+        double m3[3];
+        {
+            double z0[4], z1[4], z2[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                z0[k] = S::W == 32 ? 0.0 + v0[k] : v0[k];
+                z1[k] = S::W == 32 ? 0.0 + v1[k] : v1[k];
+                z2[k] = S::W == 32 ? 0.0 + v2[k] : v2[k];
+            }
+            m3[0] = slot_sum<TPE>(z0);
+            m3[1] = slot_sum<TPE>(z1);
+            m3[2] = slot_sum<TPE>(z2);
+        }
+        const double e2 = slot_sum<TPE>(e2k);
+        double mh = fmin(fmin(mhk[0], mhk[2]), fmin(mhk[1], mhk[3]));
+#pragma unroll
+        for (int off = TPE / 2; off > 0; off >>= 1) {
+            mh = fmin(mh, __shfl_xor_sync(0xffffffffu, mh, off));
+            fin = __shfl_xor_sync(0xffffffffu, (int)fin, off) && fin;
+        }
+        float rmsf[3];
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
             m3[f] /= N2;
-            float d3[NPT];
+            float dv[4], d3[4];
 #pragma unroll
-            for (int k = 0; k < NPT; ++k) {
+            for (int k = 0; k < 4; ++k) {
                 const double v = f == 0 ? v0[k] : (f == 1 ? v1[k] : v2[k]);
-                dv[f][k] = (float)(v - m3[f]);
-                d3[k] = dv[f][k] * dv[f][k];
+                dv[k] = val[k] ? (float)(v - m3[f]) : 0.f;
+                d3[k] = dv[k] * dv[k];
             }
-            rmsf[f] = sqrtf(quad_sum16f(d3) * (1.0f / N2));
+            rmsf[f] = sqrtf(slot_sum<TPE>(d3) * (1.0f / N2));
             const float mf = fabsf((float)m3[f]);
             const float inv = (rmsf[f] > (float)MLP_REL_FLAT * mf && rmsf[f] > 0.0f) ? 1.0f / rmsf[f] : 0.0f;
 #pragma unroll
-            for (int k = 0; k < NPT; ++k) xr[f * N2 + j + TPE * k] = __float2bfloat16(dv[f][k] * inv);
+            for (int k = 0; k < 4; ++k)
+                if (val[k]) xr[f * N2 + j + TPE * k] = __float2bfloat16(dv[k] * inv);
         }
         float sf = 0.0f;
         if (j < 3) {  // threads 0, 1, 2 of the element: the scale feature of their field
@@ -560,8 +581,9 @@ __global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused
         const float s_eta = __shfl_sync(0xffffffffu, sf, lane & ~(TPE - 1));
         const int ok = (fin && mh > a.c.PosPresTOL) ? 1 : 0;
         __syncwarp();  // the warp's feature rows complete
-        // ---- network (k_mlp_forward) on the warp's eight rows ----
-        const float y = mlp_warp_forward_rows<KP, EPW, XS, XS, W2S>(sX + warp * EPW * XS, sW1, sW2, sP32);
+        // ---- network (k_mlp_forward) on the warp's rows ----
+        const float yw = mlp_warp_forward_rows<KP, EPW, XS, XS, W2S>(sX + warp * EPW * XS, sW1, sW2, sP32);
+        const float y = __shfl_sync(0xffffffffu, yw, 4 * (lane / TPE));  // row r's output sits in quad r
         // ---- decision and modal fallback (k_indicator<NGL, true>) ----
         int nm = 1, vd = 0;
         if (live) {
@@ -571,43 +593,39 @@ __global__ void __launch_bounds__(FusedShape<NGL>::THREADS, 3) k_indicator_fused
         }
         bool clear = false;
         if (__any_sync(0xffffffffu, live && nm)) {
-            // entries (k, j), k = 0..NGL-1, of M1 = V m^T and w = M1 V^T
-            // (sensor_m1, sensor_w: the same products and sums)
-            double mrow[NGL];
+            // the modal transform, entry by entry as sensor_m1 / sensor_w
 #pragma unroll
-            for (int l = 0; l < NGL; ++l) mrow[l] = se[j * NGL + l];
-#pragma unroll
-            for (int k = 0; k < NGL; ++k) {
-                double acc = 0.0;
-#pragma unroll
-                for (int l = 0; l < NGL; ++l) acc += sV[k * NGL + l] * mrow[l];
-                sm[k * NGL + j] = acc;
+            for (int k = 0; k < 4; ++k) {
+                const int p = j + TPE * k;
+                if (val[k]) sm[p] = sensor_m1<NGL>(sV, se, p / NGL, p % NGL);
             }
             __syncwarp();
-            double w[NGL];
+            double w[4];
 #pragma unroll
-            for (int k = 0; k < NGL; ++k) {
-                double acc = 0.0;
-#pragma unroll
-                for (int l = 0; l < NGL; ++l) acc += sm[k * NGL + l] * sV[j * NGL + l];
-                w[k] = acc;
-                sw[k * NGL + j] = acc;
+            for (int k = 0; k < 4; ++k) {
+                const int p = j + TPE * k;
+                w[k] = val[k] ? sensor_w<NGL>(sV, sm, p / NGL, p % NGL) : 0.0;
+                if (val[k]) sw[p] = w[k];
             }
             __syncwarp();
-            constexpr int N = NGL - 1;
-            double z1[NPT], z2[NPT], n1[NPT], n2[NPT];
+            if constexpr (S::SCREEN) {
+                constexpr int N = NGL - 1;
+                double z1[4], z2[4], n1[4], n2[4];
 #pragma unroll
-            for (int k = 0; k < NPT; ++k) {  // entry (i, jj) = (k, j)
-                const double w2 = w[k] * w[k];
-                z1[k] = ((k == N) || (j == N)) ? w2 : 0.0;
-                z2[k] = (((k == N - 1) && (j <= N - 1)) || ((j == N - 1) && (k <= N - 1))) ? w2 : 0.0;
-                n1[k] = w2;
-                n2[k] = (k < N && j < N) ? w2 : 0.0;
+                for (int k = 0; k < 4; ++k) {
+                    const int p = j + TPE * k, i = p / NGL, jj = p % NGL;
+                    const double w2 = w[k] * w[k];
+                    z1[k] = ((i == N) || (jj == N)) ? w2 : 0.0;
+                    z2[k] = (((i == N - 1) && (jj <= N - 1)) || ((jj == N - 1) && (i <= N - 1))) ? w2 : 0.0;
+                    n1[k] = w2;
+                    n2[k] = (i < N && jj < N) ? w2 : 0.0;
+                }
+                const double Z1 = slot_sum<TPE>(z1), Z2 = slot_sum<TPE>(z2);
+                const double N1 = slot_sum<TPE>(n1), N2s = slot_sum<TPE>(n2);
+                const double thr = a.c.sensor_skip * (1.0 - 1e-6);
+                clear = N1 > a.c.ZeroTOL * (1.0 + 1e-6) && Z1 < thr * N1 && Z2 < thr * N2s;
+                clear = clear || (N1 < a.c.ZeroTOL * (1.0 - 1e-6));
             }
-            const double Z1 = quad_sum16(z1), Z2 = quad_sum16(z2), N1 = quad_sum16(n1), N2s = quad_sum16(n2);
-            const double thr = a.c.sensor_skip * (1.0 - 1e-6);
-            clear = N1 > a.c.ZeroTOL * (1.0 + 1e-6) && Z1 < thr * N1 && Z2 < thr * N2s;
-            clear = clear || (N1 < a.c.ZeroTOL * (1.0 - 1e-6));
         }
         if (live && j == 0) {
             double v = 0.0;

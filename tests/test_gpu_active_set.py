@@ -109,13 +109,15 @@ def test_indicator_needs_artificial_viscosity():
 @pytest.mark.parametrize("make", [
     lambda: problems.tsunami_member(11, sizes=(64,)),
     lambda: problems.dam_break(N=3, nel=32, seed=5),
+    lambda: problems.dam_break(N=4, nel=24, seed=6),
+    lambda: problems.tsunami_member(12, sizes=(32,), N=4),
 ])
 def test_fused_learned_pass_equals_three_passes(make):
-    """Mode 2 at N = 3 runs features, network and sensor fallback as one
-    fused kernel; mode 3 runs the three separate passes.  Same decisions,
-    same solution, bit for bit."""
+    """Mode 2 at N = 3 and 4 runs features, network and sensor fallback as
+    one fused kernel; mode 3 runs the three separate passes.  Same
+    decisions, same solution, bit for bit."""
     prob = make()
-    net = IndicatorNet.default(3)
+    net = IndicatorNet.default(prob.params.N)
     q2, st2 = _run(prob, 30, 2, net)
     q3, st3 = _run(prob, 30, 3, net)
     np.testing.assert_array_equal(q2, q3)
