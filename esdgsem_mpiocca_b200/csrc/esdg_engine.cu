@@ -537,6 +537,9 @@ class Engine {
         using T = TmaShape<NGL, tma_stages(V)>;
         auto kern = k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0, sms = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T::THREADS, T::SMEM);
@@ -615,7 +618,13 @@ class Engine {
     void launch_tma_v(const ElemArgs& ea) {
         using T = TmaShape<NGL, tma_stages(V)>;
         const int ntiles = (K + T::NE - 1) / T::NE;
-        k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+        // the plain single-mesh step runs the instance with the arena, active
+        // set, partial-dry and manufactured-source branches compiled out
+        if (!ea.elem_inst && !ea.extent && !ea.act && !ea.dry && !ea.conv)
+            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), false>
+                <<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+        else
+            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
     }
 
     template <int NGL, int R>
