@@ -779,7 +779,7 @@ def dambreak_bench(args):
 
 def reference_arm(args, ws, rank):
     """The reference's CPU path for this workload, on the host's cores: the
-    reference program with the driver's step and warm-up counts.  Nothing
+    reference program with the --steps and --warmup counts.  Nothing
     of the engine is imported or loaded in this process."""
     if rank != 0:
         return 0
