@@ -174,8 +174,10 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
     const long ex = (long)f * NGL + i;
     const double nx = a.nx[ex], ny = a.ny[ex], sc = a.scal[ex], bLx = a.bL[ex];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
+    // the instance's done flag (behind the instance table in an arena) is
+    // requested together with the traces, not before them: a face of a
+    // finished instance reads valid memory and stores nothing
     const DevState& S = a.st[inst_of(a.elem_inst, eL)];
-    if (S.done) return;
     const int ir = same ? i : NGL - 1 - i;
     const double* qe = a.q + (long)eL * 3 * N2;
     const int oL = trace_offset(sL, i, NGL);
@@ -204,8 +206,10 @@ __device__ __forceinline__ void face_flux_node(const FaceArgs& a, long gid) {
         }
         if (grad) { ghR = hL; ghuR = huL; ghvR = hvL; }
     }
+    const double bRx = a.bR[(long)f * NGL + ir];
+    if (S.done) return;
     double N0, N1, N2f;
-    es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, bLx, a.bR[(long)f * NGL + ir], N0, N1, N2f);
+    es_flux<NUMFLUX>(a.c, nx, ny, hL, huL, hvL, hR, huR, hvR, bLx, bRx, N0, N1, N2f);
     const double s = sc;
     const double v0 = s * a.c.geomFace * N0, v1 = s * a.c.geomFace * N1, v2 = s * a.c.geomFace * N2f;
     if (SIDEOUT) {
@@ -277,7 +281,9 @@ __device__ __forceinline__ void face_visc_node(long gid, const int4* __restrict_
     const int f = (int)(gid / NGL), i = (int)(gid % NGL);
     const int4 t = ftab[f];
     const int eL = t.x, eR = t.y, sL = t.z & 3, sR = (t.z >> 2) & 3, same = (t.z >> 4) & 1;
-    if (st[inst_of(elem_inst, eL)].done) return;
+    // the done flag (behind the instance table in an arena) and the active
+    // flags are requested together
+    const bool done = st[inst_of(elem_inst, eL)].done;
     const long ex = (long)f * NGL + i;
     double N0 = 0.0, N1 = 0.0;
     // Active set: only faces of flagged elements are read.  A face with a
@@ -289,6 +295,7 @@ __device__ __forceinline__ void face_visc_node(long gid, const int4* __restrict_
         if (!aL && !aR) return;
         need = aL && aR;
     }
+    if (done) return;
     if (eR >= 0 && need) {
         const int inc = same ? i : NGL - 1 - i;
         const long oL = (long)eL * 2 * N2 + trace_offset(sL, i, NGL);
