@@ -170,6 +170,7 @@ class Engine {
     double *DcFD = nullptr, *DupFD = nullptr, *DdnFD = nullptr;
     bool pd_copied = false;
     int list_grid = 0;                        // persistent grid of the list kernels
+    int face_list_grid = 0;                   // grid of the viscous face kernel over the listed elements' faces
     int ind_grid[3] = {1, 1, 1};              // persistent grids of the indicator (modal, learned, fused)
 
     // step graph
@@ -761,8 +762,9 @@ class Engine {
             ea.act = act; ea.alist = alist; ea.acount = act + K;
             launch_elem_plain<NGL>(ea);
             k_grad_list<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
-            const long n = (long)F * NGL;
-            launch_face_visc<NGL>(n, act, extent);
+            // the viscous face fluxes of the listed elements' faces only
+            k_face_visc_list<NGL><<<face_list_grid, 256, 0, stream>>>(side, ftab, nx, ny, scal, GX, GY, VP, SPV,
+                                                                      elem_inst, st, geomFace, act, alist, act + K);
             k_element_av2<NGL><<<list_grid, S::THREADS, 0, stream>>>(ea);
             launches += 3;
         } else if (!AV) {
@@ -843,6 +845,10 @@ class Engine {
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy (list kernels)");
         list_grid = std::max(1, std::min(std::max(1, std::min(a2, gr)) * sms, (K + S::NE - 1) / S::NE));
+        int fv = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fv, k_face_visc_list<NGL>, 256, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "occupancy (viscous face list)");
+        face_list_grid = std::max(1, std::min(std::max(1, fv) * sms, (int)(((long)K * 4 * NGL + 255) / 256)));
         int o0 = 0, o1 = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o0, k_indicator<NGL, false>, IndShape<NGL>::THREADS, 0);
         if (e == cudaSuccess)

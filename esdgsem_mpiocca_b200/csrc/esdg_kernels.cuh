@@ -334,6 +334,37 @@ __global__ void __launch_bounds__(256, STRIDE ? 4 : 1) k_face_visc(int F, const 
     }
 }
 
+// The viscous face fluxes of the active set only: the faces of the listed
+// (flagged) elements alist[0 .. *acount), one thread per face node, grid
+// stride.  A face of a listed element e is evaluated by e when e is its
+// master side or when its master side is not flagged (then not listed), so
+// each such face is evaluated exactly once, by face_visc_node (the same
+// arithmetic as k_face_visc); faces with no flagged side are read by no
+// one and left alone, as k_face_visc leaves them.  One thread per node of
+// the listed elements' sides instead of one per face node of the mesh.
+template <int NGL>
+__global__ void __launch_bounds__(256) k_face_visc_list(const int4* __restrict__ side, const int4* __restrict__ ftab,
+                                                        const double* __restrict__ nxa, const double* __restrict__ nya,
+                                                        const double* __restrict__ scal, const double* __restrict__ GX,
+                                                        const double* __restrict__ GY, const double* __restrict__ VP,
+                                                        double* __restrict__ SPV, const int* __restrict__ elem_inst,
+                                                        const DevState* __restrict__ st, double geomFace,
+                                                        const int* __restrict__ act, const int* __restrict__ alist,
+                                                        const int* __restrict__ acount) {
+    const long n = (long)(*acount) * 4 * NGL;
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const int e = alist[k / (4 * NGL)];
+        const int sd = (int)((k / NGL) % 4), i = (int)(k % NGL);
+        const int f = side[(long)e * 4 + sd].x;
+        const int4 t = ftab[f];
+        // the master side evaluates the face (an element that is both sides
+        // of a face, on a periodic strip, through its master side only);
+        // the slave side only when the master is not flagged
+        if (t.x == e ? sd != (t.z & 3) : act[t.x] != 0) continue;
+        face_visc_node<NGL>((long)f * NGL + i, ftab, nxa, nya, scal, GX, GY, VP, SPV, elem_inst, st, geomFace, act);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Element kernels.
 // ---------------------------------------------------------------------------
