@@ -576,6 +576,9 @@ class Engine {
         using P = PairShape<NGL>;
         auto kern = k_element_pair<NGL, pair_min_blocks(V)>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_element_pair<NGL, pair_min_blocks(V), false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0, sms = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::THREADS, P::SMEM);
@@ -592,7 +595,11 @@ class Engine {
     void launch_pair_v(const ElemArgs& ea) {
         using P = PairShape<NGL>;
         const int ntiles = (K + P::NE - 1) / P::NE;
-        k_element_pair<NGL, pair_min_blocks(V)><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
+        if (!ea.elem_inst && !ea.extent && !ea.act && !ea.dry && !ea.conv)
+            k_element_pair<NGL, pair_min_blocks(V), false>
+                <<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
+        else
+            k_element_pair<NGL, pair_min_blocks(V)><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
     }
 
     template <int NGL>
