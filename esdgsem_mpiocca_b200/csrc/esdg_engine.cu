@@ -539,7 +539,10 @@ class Engine {
         auto kern = k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), false>,
+            e = cudaFuncSetAttribute(k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), 0>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0, sms = 0;
@@ -571,13 +574,24 @@ class Engine {
         return 0;
     }
 
+    // Instance of the node-per-thread and two-nodes-per-thread kernels a
+    // launch needs: 0 the plain single mesh, 2 an arena or active set
+    // without the partial-dry treatment and manufactured source, 1 all.
+    static int elem_gen(const ElemArgs& ea) {
+        if (!ea.elem_inst && !ea.extent && !ea.act && !ea.dry && !ea.conv) return 0;
+        return (!ea.dry && !ea.conv) ? 2 : 1;
+    }
+
     template <int NGL, int V>
     int setup_pair_variant() {
         using P = PairShape<NGL>;
         auto kern = k_element_pair<NGL, pair_min_blocks(V)>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_element_pair<NGL, pair_min_blocks(V), false>,
+            e = cudaFuncSetAttribute(k_element_pair<NGL, pair_min_blocks(V), 0>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_element_pair<NGL, pair_min_blocks(V), 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0, sms = 0;
@@ -595,11 +609,13 @@ class Engine {
     void launch_pair_v(const ElemArgs& ea) {
         using P = PairShape<NGL>;
         const int ntiles = (K + P::NE - 1) / P::NE;
-        if (!ea.elem_inst && !ea.extent && !ea.act && !ea.dry && !ea.conv)
-            k_element_pair<NGL, pair_min_blocks(V), false>
-                <<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
+        const int gen = elem_gen(ea);
+        if (gen == 0)
+            k_element_pair<NGL, pair_min_blocks(V), 0><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
+        else if (gen == 2)
+            k_element_pair<NGL, pair_min_blocks(V), 2><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
         else
-            k_element_pair<NGL, pair_min_blocks(V)><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
+            k_element_pair<NGL, pair_min_blocks(V), 1><<<tma_grid[PAIR_FIRST + V], P::THREADS, P::SMEM, stream>>>(ea, ntiles);
     }
 
     template <int NGL>
@@ -626,13 +642,14 @@ class Engine {
     void launch_tma_v(const ElemArgs& ea) {
         using T = TmaShape<NGL, tma_stages(V)>;
         const int ntiles = (K + T::NE - 1) / T::NE;
-        // the plain single-mesh step runs the instance with the arena, active
-        // set, partial-dry and manufactured-source branches compiled out
-        if (!ea.elem_inst && !ea.extent && !ea.act && !ea.dry && !ea.conv)
-            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), false>
-                <<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+        // the instance with the branches this step does not need compiled out
+        const int gen = elem_gen(ea);
+        if (gen == 0)
+            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), 0><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+        else if (gen == 2)
+            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), 2><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
         else
-            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V)><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
+            k_element_tma<NGL, tma_min_blocks(V), tma_stages(V), 1><<<tma_grid[V], T::THREADS, T::SMEM, stream>>>(ea, ntiles);
     }
 
     template <int NGL, int R>

@@ -29,13 +29,13 @@ struct PairShape : TileLayout<NGL, TmaShape<NGL>::NE - TmaShape<NGL>::NE % 2> {
 constexpr int PAIR_VARIANTS = 2;
 __host__ __device__ constexpr int pair_min_blocks(int v) { return v == 0 ? 3 : 4; }
 
-// GEN = false: the plain single-mesh step (no arena, active set, partial-dry
-// treatment or manufactured source), those branches compiled out.
-template <int NGL, int MINB, bool GEN = true>
+// GEN as for k_element_tma: 0 plain single mesh, 2 arena or active set
+// without partial-dry treatment or manufactured source, 1 everything.
+template <int NGL, int MINB, int GEN = 1>
 __global__ void __launch_bounds__(PairShape<NGL>::THREADS, MINB) k_element_pair(ElemArgs a, int ntiles) {
     using P = PairShape<NGL>;
     constexpr int N2 = P::N2, NE = P::NE, H = P::HALF, ST = P::ST;
-    if (GEN && a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
+    if (GEN != 0 && a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     extern __shared__ __align__(128) double smem[];
     double* stage = smem;
     double* su = smem + ST * P::STAGE_DOUBLES;
@@ -82,9 +82,9 @@ __global__ void __launch_bounds__(PairShape<NGL>::THREADS, MINB) k_element_pair(
         for (int k = 0; k < 2; ++k) {
             e[k] = e0 + el0 + k * H;
             const bool inb = e[k] < a.K;
-            ins[k] = (GEN && inb) ? inst_of(a.elem_inst, e[k]) : 0;
+            ins[k] = (GEN != 0 && inb) ? inst_of(a.elem_inst, e[k]) : 0;
             active[k] = inb && !a.st[ins[k]].done;
-            to_list[k] = GEN && active[k] && a.act && a.act[e[k]] != 0;
+            to_list[k] = GEN != 0 && active[k] && a.act && a.act[e[k]] != 0;
             dt[k] = (active[k] && a.mode != 2) ? a.st[ins[k]].dt : 0.0;
         }
         // every thread waits for the tile; a copy that never lands makes the
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(PairShape<NGL>::THREADS, MINB) k_element_pair(
             double r0 = -J * e1;
             double r1 = -J * e2 - a.c.g * h[k] * sBx[s];
             double r2 = -J * e3 - a.c.g * h[k] * sBy[s];
-            if (GEN && a.dry && a.dry[e[k]])
+            if (GEN == 1 && a.dry && a.dry[e[k]])
                 pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sq + el * 3 * N2, a.Bn + (long)e[k] * N2, eta, xi, sYe[s],
                                sYx[s], sXe[s], sXx[s], J, r1, r2);
             // lift: sides 0/2 first, then 1/3, from the tile's element-side
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(PairShape<NGL>::THREADS, MINB) k_element_pair(
                     r2 += J * fp[2 * NGL] + J * db;
                 }
             }
-            if (GEN && a.conv) add_conv_source(a, a.st[ins[k]], (long)e[k] * N2 + nd, sBx[s], sBy[s], r0, r1, r2);
+            if (GEN == 1 && a.conv) add_conv_source(a, a.st[ins[k]], (long)e[k] * N2 + nd, sBx[s], sBy[s], r0, r1, r2);
             const long qid = (long)e[k] * 3 * N2 + nd;
             if (a.mode == 2 || to_list[k]) {
                 a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;

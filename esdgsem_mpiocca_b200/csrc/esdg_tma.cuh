@@ -191,13 +191,15 @@ __device__ __forceinline__ void tma_issue_tile(const ElemArgs& a, int t, double*
 
 // Persistent flux-differencing volume term + surface lift + RK update
 // (same operations as k_element), tiles double-buffered through TMA.
-// GEN = false: the plain single-mesh step (no arena, active set, partial-dry
-// treatment or manufactured source), those branches compiled out.
-template <int NGL, int MINB, int NST, bool GEN = true>
+// GEN = 0: the plain single-mesh step (no arena, active set, partial-dry
+// treatment or manufactured source), those branches compiled out; 2: an
+// arena or active set without the partial-dry treatment and manufactured
+// source; 1: everything.
+template <int NGL, int MINB, int NST, int GEN = 1>
 __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(ElemArgs a, int ntiles) {
     using S = TmaShape<NGL, NST>;
     constexpr int N2 = S::N2, NE = S::NE, ST = S::STAGES;
-    if (GEN && a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
+    if (GEN != 0 && a.extent) ntiles = min(ntiles, (a.extent[0] + NE - 1) / NE);
     extern __shared__ __align__(128) double smem[];
     double* stage = smem;
     double* su = smem + ST * S::STAGE_DOUBLES;
@@ -234,9 +236,9 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
         const int e0 = t * NE;
         const int e = e0 + el;
         const bool inb = e < a.K;
-        const int ins = (GEN && inb) ? inst_of(a.elem_inst, e) : 0;
+        const int ins = (GEN != 0 && inb) ? inst_of(a.elem_inst, e) : 0;
         const bool active = inb && !a.st[ins].done;
-        const bool to_list = GEN && active && a.act && a.act[e] != 0;
+        const bool to_list = GEN != 0 && active && a.act && a.act[e] != 0;
         const double dt = (active && a.mode != 2) ? a.st[ins].dt : 0.0;
         // every thread waits for the tile; a copy that never lands makes the
         // whole CTA leave together (uniform decision) with an error status
@@ -293,7 +295,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
             double r0 = -J * d1;
             double r1 = -J * d2 - a.c.g * h * sBx[s];
             double r2 = -J * d3 - a.c.g * h * sBy[s];
-            if (GEN && a.dry && a.dry[e])
+            if (GEN == 1 && a.dry && a.dry[e])
                 pd_volume<NGL>(a.c, a.Dc, a.Dup, a.Ddn, sq + el * 3 * N2, a.Bn + (long)e * N2, eta, xi, ye, yx, xe, xx,
                                J, r1, r2);
             // lift: sides 0/2 first, then 1/3, from the tile's element-side
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(TmaShape<NGL>::THREADS, MINB) k_element_tma(El
                     r2 += J * fp[2 * NGL] + J * db;
                 }
             }
-            if (GEN && a.conv) add_conv_source(a, a.st[ins], (long)e * N2 + nd, sBx[s], sBy[s], r0, r1, r2);
+            if (GEN == 1 && a.conv) add_conv_source(a, a.st[ins], (long)e * N2 + nd, sBx[s], sBy[s], r0, r1, r2);
             const long qid = (long)e * 3 * N2 + nd;
             if (a.mode == 2 || to_list) {
                 a.Qt[qid] = r0; a.Qt[qid + N2] = r1; a.Qt[qid + 2 * N2] = r2;
