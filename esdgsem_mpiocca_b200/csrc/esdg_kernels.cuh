@@ -259,8 +259,15 @@ __global__ void __launch_bounds__(256, STRIDE ? 4 : 1) k_face_flux(FaceArgs a) {
     long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long all = (long)a.F * NGL;
     if (!STRIDE) {
-        if (gid >= all || (a.extent && gid >= (long)a.extent[1] * NGL)) return;
-        face_flux_node<NGL, NUMFLUX, AV, SIDEOUT>(a, gid);
+        // Descending face order.  Face ids follow the element order (a face
+        // is numbered by the first element that has it) and the element
+        // kernels walk their tiles upwards, so the first faces taken here
+        // read the traces the element kernel wrote last, and the fluxes
+        // written last are those of the first tiles the next element kernel
+        // reads: both still in L2.
+        const long n = a.extent ? min(all, (long)a.extent[1] * NGL) : all;
+        if (gid >= n) return;
+        face_flux_node<NGL, NUMFLUX, AV, SIDEOUT>(a, n - 1 - gid);
     } else {
         const long n = a.extent ? min(all, (long)a.extent[1] * NGL) : all;
         for (; gid < n; gid += (long)gridDim.x * blockDim.x) face_flux_node<NGL, NUMFLUX, AV, SIDEOUT>(a, gid);

@@ -111,6 +111,11 @@ def test_indicator_needs_artificial_viscosity():
     lambda: problems.dam_break(N=3, nel=32, seed=5),
     lambda: problems.dam_break(N=4, nel=24, seed=6),
     lambda: problems.tsunami_member(12, sizes=(32,), N=4),
+    # element counts whose last tile of the fused pass ends inside a warp
+    # (441 = 6 * 64 + 57 at N = 3, 529 = 16 * 32 + 17 at N = 4): idle
+    # element slots next to live ones in the same network tile
+    lambda: problems.dam_break(N=3, nel=21, seed=5),
+    lambda: problems.dam_break(N=4, nel=23, seed=6),
 ])
 def test_fused_learned_pass_equals_three_passes(make):
     """Mode 2 at N = 3 and 4 runs features, network and sensor fallback as
