@@ -17,6 +17,7 @@ value is the sum over ranks divided by the slowest rank's time.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -115,25 +116,39 @@ def dist_env():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons while timing."""
+    """nvidia-smi sampling of SM clocks and throttle reasons while timing.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Samples every `interval_ms`.  When the caller sets `window` (host times
+    bracketing the timed region, device work included) only the samples
+    taken inside it are kept; `in_window` counts them (a region of a few
+    tens of milliseconds holds one or two)."""
+
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, interval_ms: int = 200):
         self.gpu = gpu_index
+        self.interval = interval_ms
         self.proc = None
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
         time.sleep(0.3)
         return self
+
+    @staticmethod
+    def _stamp(text):
+        try:
+            return datetime.datetime.strptime(text.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
 
     def __exit__(self, *a):
         self.result = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
@@ -145,23 +160,31 @@ class Clocks:
         except Exception:
             self.proc.kill()
             out = ""
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in out.splitlines():
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
+                rows.append((self._stamp(f[0]), float(f[1]), float(f[2]), float(f[3]), f[5:9]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if sm:
-            self.result = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                           "samples": len(sm)}
+        if self.window is not None:
+            t0, t1 = self.window
+            inside = [r for r in rows if r[0] is not None and t0 <= r[0] <= t1]
+            self.result["in_window"] = len(inside)
+            # a region shorter than the interval: the sample nearest to it
+            if not inside and rows:
+                mid = 0.5 * (t0 + t1)
+                inside = [min((r for r in rows if r[0] is not None), key=lambda r: abs(r[0] - mid),
+                              default=rows[-1])]
+            rows = inside
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {nm for r in rows for nm, v in zip(names, r[4]) if v.lower() == "active"}
+        if rows:
+            self.result.update({"sm_mhz": statistics.median(r[1] for r in rows),
+                                "sm_max_mhz": max(r[2] for r in rows), "reasons": sorted(reasons),
+                                "power_w": statistics.median(r[3] for r in rows), "samples": len(rows)})
         return False
 
 
@@ -354,12 +377,14 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with Clocks(local) as ck:
+    with Clocks(local, 20) as ck:
+        tw0 = time.time()
         with torch.cuda.stream(stream):
             e0.record(stream)
             t_sim, nsteps_done = s.dc.advance(args.steps, 1e9)
             e1.record(stream)
         torch.cuda.synchronize()
+        ck.window = (tw0, time.time())
     if dist:
         dist.barrier()
     launches = s.dc.kernel_launches() - launches0
@@ -395,6 +420,18 @@ def main():
         "gpu_launches": int(launches),
         "clocks": ck.result,
     }
+    # ---- the same step loop for about a second, outside the timed region:
+    # the clocks and power a sustained run settles at, and its step time ----
+    nsus = max(args.steps, int(1000.0 / max(ms / args.steps, 0.05)))
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local, 50) as ck2:
+        with torch.cuda.stream(stream):
+            e2.record(stream)
+            s.dc.advance(nsus, 1e9)
+            e3.record(stream)
+        torch.cuda.synchronize()
+    line["clocks_sustained"] = dict(ck2.result, steps=nsus, ms_per_step=e2.elapsed_time(e3) / nsus)
     s.close()
     # ---- the batched+learned half of the metric: the 256-member tsunami
     # ensemble, batched with the learned indicator vs one at a time plain ----

@@ -56,3 +56,46 @@ def test_committed_traffic_lines_parse():
         if "traffic_bytes_per_launch:" in text:
             assert title in bench.ELEMENT_KERNELS_N4, fn
             assert bench.profiled_traffic(title) > 0
+
+
+class _FakeSmi:
+    """nvidia-smi's CSV lines, as the sampler reads them at exit."""
+
+    def __init__(self, lines):
+        self.lines = lines
+
+    def terminate(self):
+        pass
+
+    def communicate(self, timeout=None):
+        return "\n".join(self.lines), ""
+
+
+def test_clocks_keep_the_samples_inside_the_timed_window():
+    import datetime
+    import time
+    now = time.time()
+
+    def row(dt, mhz, watts, cap):
+        stamp = datetime.datetime.fromtimestamp(now + dt).strftime("%Y/%m/%d %H:%M:%S.%f")[:-3]
+        return f"{stamp}, {mhz}, 1965, {watts}, 0x0, Not Active, Not Active, Not Active, {cap}"
+
+    lines = [row(-0.2, 1965, 300.0, "Not Active"), row(0.01, 1800, 950.0, "Active"),
+             row(0.5, 1700, 990.0, "Active")]
+    c = bench.Clocks(0)
+    c.proc = _FakeSmi(lines)
+    c.window = (now, now + 0.03)
+    c.__exit__(None, None, None)
+    assert c.result["in_window"] == 1 and c.result["samples"] == 1
+    assert c.result["sm_mhz"] == 1800.0 and c.result["reasons"] == ["sw_power_cap"]
+    # no sample inside a short window: the nearest one, reported as such
+    c = bench.Clocks(0)
+    c.proc = _FakeSmi(lines)
+    c.window = (now + 0.1, now + 0.12)
+    c.__exit__(None, None, None)
+    assert c.result["in_window"] == 0 and c.result["sm_mhz"] == 1800.0
+    # no window: every sample
+    c = bench.Clocks(0)
+    c.proc = _FakeSmi(lines)
+    c.__exit__(None, None, None)
+    assert c.result["samples"] == 3 and c.result["sm_mhz"] == 1800.0
